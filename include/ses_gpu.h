@@ -1,0 +1,161 @@
+/* ses_gpu.h -- C ABI of the B200 split-operator (Strang) TDSE step.
+ *
+ * Drop-in boundary for the reference core's propagator / propagator-tables /
+ * fft3 call surface (parkyere/ShoeridingerEquationSolver).  The reference has
+ * no FFI layer of its own: callers use C++ module interfaces.  Each entry point
+ * below names the reference interface it replaces (file:line inside the
+ * reference project).  Plain pointers and sizes only; no exceptions cross
+ * this boundary; every call returns a ses_status and, on failure, leaves a
+ * message for ses_last_error() on the calling thread.
+ *
+ * Data conventions (same as the reference):
+ *   - complex fields are interleaved (re, im) doubles on the host, flat
+ *     x-fastest order, index i + nx*(j + ny*k)       (core/src/grid.ixx:20-30)
+ *   - grids are periodic: spacing = (xmax - xmin)/n  (core/src/grid.ixx:4-18)
+ *   - forward FFT unnormalised with e^{-}, inverse carries 1/N
+ *                                                     (core/src/fft.ixx:14-18)
+ *   - 2D scenes are Grid3D with nz = 1, 1D is nx x 1 x 1 (axes of length 1
+ *     are left untransformed; wavenumber 0)           (core/src/spectral.ixx:14-23)
+ *
+ * Supported axis lengths: 2^a 3^b 5^c up to 4096 (the reference accepts powers
+ * of two only and throws std::invalid_argument otherwise; here other lengths
+ * return SES_EINVAL).
+ *
+ * Threading: calls on one handle must be serialised by the caller (like the
+ * reference engine, vk_compute.ixx:272-274); distinct handles are independent.
+ * All device work of a handle is ordered on that handle's CUDA stream.
+ */
+#ifndef SES_GPU_H
+#define SES_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SES_API __attribute__((visibility("default")))
+#else
+#define SES_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ses_status {
+    SES_OK = 0,
+    SES_EINVAL = 1,     /* bad size, radix, pointer or argument */
+    SES_ENOMEM = 2,     /* device allocation failed or memory budget exceeded */
+    SES_ETIMEDOUT = 3,  /* a bounded wait expired */
+    SES_EDEVICE = 4,    /* CUDA error; the handle should be destroyed */
+    SES_EBUSY = 5,      /* resource busy (serving queue full) */
+    SES_ENOTFOUND = 6   /* unknown request id */
+} ses_status;
+
+/* SES_C128: plain FP64 path (complex128 psi and tables).
+ * SES_C64:  complex64 psi and FFT arithmetic; phase tables built in FP64,
+ *           diagonal multiplies and all reductions in FP64. */
+typedef enum ses_precision { SES_C128 = 0, SES_C64 = 1 } ses_precision;
+
+/* Grid1D (core/src/grid.ixx:10-17) */
+typedef struct ses_axis {
+    double xmin;
+    double xmax;
+    int32_t n;
+} ses_axis;
+
+/* Grid3D (core/src/grid.ixx:22-30) */
+typedef struct ses_grid_desc {
+    ses_axis x, y, z;
+} ses_grid_desc;
+
+typedef struct ses_solver* ses_handle;
+
+/* Observables of the resident psi at a step boundary, FP64 accumulation. */
+typedef struct ses_observables {
+    double norm;         /* sum |psi|^2 dV                        (core/src/field.ixx:68-74) */
+    double energy;       /* <V> + <T>, each term normalised separately
+                                                          (core/src/observables.ixx:202-234) */
+    double energy_v;     /* sum V|psi|^2 / sum |psi|^2                                 */
+    double energy_t;     /* sum k^2/(2m)|phi|^2 / sum |phi|^2, phi = FFT(psi)          */
+    double p_range;      /* absolute sum |psi|^2 dV over cells with x in [xlo, xhi)
+                                                          (core/src/observables.ixx:121-130,
+                                                   scenario/src/tunneling_director.ixx:54-85) */
+    double mean_pos[3];  /* (core/src/observables.ixx:134-153) */
+    double sigma_pos[3]; /* (core/src/observables.ixx:155-178) */
+    double mean_mom[3];  /* (core/src/observables.ixx:180-199) */
+} ses_observables;
+
+/* ---- library ---- */
+SES_API const char* ses_version(void);
+/* Message of the last failing call on this thread ("" when none). */
+SES_API const char* ses_last_error(void);
+SES_API ses_status ses_device_count(int* out);
+
+/* ---- SplitOperator3D surface (core/src/propagator.ixx:68-134) ----
+ * ses_gpu_create replaces SplitOperator3D(const Grid3D&, const std::vector<double>& V,
+ * double dt, double mass = 1.0) (propagator.ixx:72-101) together with the
+ * reference GPU Engine::initialize(ctx, grid, kernels, V, dt, psi0, mass)
+ * (solver/src/vk_engine.ixx:173-580): it builds the FP64 phase tables on the
+ * device and uploads psi0 (NULL -> zero field).  V has nx*ny*nz doubles.
+ * SplitOperator1D (propagator.ixx:21-66) is the same call with ny = nz = 1
+ * and mass = 1. */
+SES_API ses_status ses_gpu_create(const ses_grid_desc* grid, ses_precision prec, double dt, double mass,
+                          const double* V, const double* psi0, ses_handle* out);
+/* Engine::destroy (vk_engine.ixx) */
+SES_API ses_status ses_gpu_destroy(ses_handle h);
+/* Engine::set_potential (vk_engine.ixx): rebuild the potential phase table. */
+SES_API ses_status ses_gpu_set_potential(ses_handle h, const double* V);
+/* Engine::set_absorber(mask) (vk_engine.ixx:880-941): real per-cell mask,
+ * N doubles; NULL clears it.  A mask that is an exact product of per-axis
+ * profiles (absorbing_mask, potential.ixx:216-233) is stored as three 1D
+ * profiles; any other mask is stored in full. */
+SES_API ses_status ses_gpu_set_absorber(ses_handle h, const double* mask);
+/* Separable absorber: mask(i,j,k) = mx[i] * my[j] * mz[k]. */
+SES_API ses_status ses_gpu_set_absorber_separable(ses_handle h, const double* mx, const double* my,
+                                          const double* mz);
+/* SplitOperator3D::step(Field3D&, int nsteps) (propagator.ixx:110-119) on the
+ * resident psi; with absorb != 0 psi is multiplied by the mask after EVERY
+ * step (Engine::step(n, absorb), vk_engine.ixx:597-636).  Interior half-kicks
+ * are merged into full kicks, so psi is in real space only at batch ends.
+ * Asynchronous: returns once the work is queued on the handle's stream. */
+SES_API ses_status ses_gpu_step(ses_handle h, int nsteps, int absorb);
+/* fft(Field3D&) / ifft(Field3D&) (core/src/fft.ixx:102-188) on the resident
+ * psi: direction 0 = forward (unnormalised), 1 = inverse (1/N). */
+SES_API ses_status ses_gpu_fft3(ses_handle h, int direction);
+/* half_potential_phase() / kinetic_phase() (propagator.ixx:103-108): the
+ * full-N complex128 tables cis(-V dt/2) and cis(-(kx^2+ky^2+kz^2)/(2m) dt),
+ * evaluated in FP64 on the device.  Either pointer may be NULL. */
+SES_API ses_status ses_gpu_tables(ses_handle h, double* half_v, double* kin);
+/* dt() (propagator.ixx:103) */
+SES_API ses_status ses_gpu_dt(ses_handle h, double* dt);
+/* norm_sq, mean_energy, probability_in_range, mean_position, sigma_position,
+ * mean_momentum of the resident psi (observables.ixx:121-234), with xlo/xhi
+ * the x-interval of p_range.  Blocks until the values are on the host. */
+SES_API ses_status ses_gpu_observe(ses_handle h, double xlo, double xhi, ses_observables* out);
+/* Engine::readback / upload_state (vk_engine.ixx:2136-2155, 1083-1089,
+ * 2413-2421): interleaved complex128 host arrays of N elements (the C64 path
+ * rounds on upload and widens on readback).  Both block until done. */
+SES_API ses_status ses_gpu_read_psi(ses_handle h, double* psi_out);
+SES_API ses_status ses_gpu_write_psi(ses_handle h, const double* psi_in);
+/* Wait for the handle's queued work; the wait is bounded by timeout_ms
+ * (<= 0: 10 s, the reference's fence limit vk_compute.ixx:297-327) and
+ * returns SES_ETIMEDOUT when it expires. */
+SES_API ses_status ses_gpu_sync(ses_handle h, int timeout_ms);
+/* Use an external cudaStream_t (NULL: the handle's own stream). */
+SES_API ses_status ses_gpu_set_stream(ses_handle h, void* cuda_stream);
+/* Device pointer and byte size of the resident psi (complex128 or complex64,
+ * x-fastest), for callers that keep data on the device. */
+SES_API ses_status ses_gpu_psi_device(ses_handle h, void** dptr, size_t* bytes);
+/* Device bytes held by the handle. */
+SES_API ses_status ses_gpu_footprint(ses_handle h, size_t* bytes);
+
+/* ---- fft surface on host arrays (core/src/fft.ixx:75-188) ----
+ * fft(std::vector<cd>&) / ifft(...) and fft(Field3D&) / ifft(Field3D&):
+ * n[3] = (nx, ny, nz), data = interleaved complex128, transformed in place
+ * through the device. */
+SES_API ses_status ses_fft3_host(const int32_t* n, ses_precision prec, double* data, int inverse);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SES_GPU_H */

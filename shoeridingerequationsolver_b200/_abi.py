@@ -1,0 +1,125 @@
+"""ctypes binding of the C ABI in include/ses_gpu.h (libses_b200.so).
+
+The library is built in-tree (``python shoeridingerequationsolver_b200/build.py``).
+There is no fallback: if the shared library is missing or fails to load,
+importing this module raises ``ImportError``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libses_b200.so"
+
+SES_OK, SES_EINVAL, SES_ENOMEM, SES_ETIMEDOUT, SES_EDEVICE, SES_EBUSY, SES_ENOTFOUND = range(7)
+SES_C128, SES_C64 = 0, 1
+
+# every symbol include/ses_gpu.h declares
+EXPORTS = [
+    "ses_version", "ses_last_error", "ses_device_count",
+    "ses_gpu_create", "ses_gpu_destroy", "ses_gpu_set_potential", "ses_gpu_set_absorber",
+    "ses_gpu_set_absorber_separable", "ses_gpu_step", "ses_gpu_fft3", "ses_gpu_tables",
+    "ses_gpu_dt", "ses_gpu_observe", "ses_gpu_read_psi", "ses_gpu_write_psi", "ses_gpu_sync",
+    "ses_gpu_set_stream", "ses_gpu_psi_device", "ses_gpu_footprint", "ses_fft3_host",
+]
+
+
+class Axis(C.Structure):
+    _fields_ = [("xmin", C.c_double), ("xmax", C.c_double), ("n", C.c_int32)]
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("x", Axis), ("y", Axis), ("z", Axis)]
+
+
+class Observables(C.Structure):
+    _fields_ = [("norm", C.c_double), ("energy", C.c_double), ("energy_v", C.c_double),
+                ("energy_t", C.c_double), ("p_range", C.c_double),
+                ("mean_pos", C.c_double * 3), ("sigma_pos", C.c_double * 3),
+                ("mean_mom", C.c_double * 3)]
+
+    def as_dict(self) -> dict:
+        return {
+            "norm": self.norm, "energy": self.energy, "energy_v": self.energy_v,
+            "energy_t": self.energy_t, "p_range": self.p_range,
+            "mean_pos": list(self.mean_pos), "sigma_pos": list(self.sigma_pos),
+            "mean_mom": list(self.mean_mom),
+        }
+
+
+class SesError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"ses status {status}: {msg}")
+        self.status = status
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built; run python shoeridingerequationsolver_b200/build.py")
+    lib = C.CDLL(str(LIB_PATH))
+    dp, vp, hp = C.POINTER(C.c_double), C.c_void_p, C.c_void_p
+    st = C.c_int
+    sig = {
+        "ses_version": ([], C.c_char_p),
+        "ses_last_error": ([], C.c_char_p),
+        "ses_device_count": ([C.POINTER(C.c_int)], st),
+        "ses_gpu_create": ([C.POINTER(GridDesc), C.c_int, C.c_double, C.c_double, dp, dp,
+                            C.POINTER(hp)], st),
+        "ses_gpu_destroy": ([hp], st),
+        "ses_gpu_set_potential": ([hp, dp], st),
+        "ses_gpu_set_absorber": ([hp, dp], st),
+        "ses_gpu_set_absorber_separable": ([hp, dp, dp, dp], st),
+        "ses_gpu_step": ([hp, C.c_int, C.c_int], st),
+        "ses_gpu_fft3": ([hp, C.c_int], st),
+        "ses_gpu_tables": ([hp, dp, dp], st),
+        "ses_gpu_dt": ([hp, dp], st),
+        "ses_gpu_observe": ([hp, C.c_double, C.c_double, C.POINTER(Observables)], st),
+        "ses_gpu_read_psi": ([hp, vp], st),
+        "ses_gpu_write_psi": ([hp, vp], st),
+        "ses_gpu_sync": ([hp, C.c_int], st),
+        "ses_gpu_set_stream": ([hp, vp], st),
+        "ses_gpu_psi_device": ([hp, C.POINTER(vp), C.POINTER(C.c_size_t)], st),
+        "ses_gpu_footprint": ([hp, C.POINTER(C.c_size_t)], st),
+        "ses_fft3_host": ([C.POINTER(C.c_int32), C.c_int, dp, C.c_int], st),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    return lib.ses_last_error().decode()
+
+
+def check(status: int) -> None:
+    """Map a ses_status to the reference's error behaviour: invalid sizes raise
+    ValueError (std::invalid_argument in core/src/fft.ixx:42-44), exhausted
+    memory MemoryError, an expired bounded wait TimeoutError, device errors
+    SesError."""
+    if status == SES_OK:
+        return
+    msg = last_error()
+    if status == SES_EINVAL:
+        raise ValueError(msg)
+    if status == SES_ENOMEM:
+        raise MemoryError(msg)
+    if status == SES_ETIMEDOUT:
+        raise TimeoutError(msg)
+    raise SesError(status, msg)
+
+
+def grid_desc(grid) -> GridDesc:
+    return GridDesc(Axis(grid.x.xmin, grid.x.xmax, grid.x.n), Axis(grid.y.xmin, grid.y.xmax, grid.y.n),
+                    Axis(grid.z.xmin, grid.z.xmax, grid.z.n))
+
+
+def device_count() -> int:
+    c = C.c_int(0)
+    st = lib.ses_device_count(C.byref(c))
+    return c.value if st == SES_OK else 0

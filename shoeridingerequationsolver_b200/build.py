@@ -1,0 +1,62 @@
+"""Build the product library libses_b200.so (sm_100a) in-tree with nvcc.
+
+Usage: ``python shoeridingerequationsolver_b200/build.py [--verbose-ptxas]`` (runs
+without importing the package, which needs the built library).
+The library exports exactly the C ABI declared in ``include/ses_gpu.h``.
+"""
+
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIB = PKG / "libses_b200.so"
+SOURCES = ["ses_gpu.cu"]
+HEADERS = ["ses_fft.cuh", "ses_pass.cuh"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-shared",
+         "--expt-relaxed-constexpr", "-Xcompiler", "-fvisibility=hidden"]
+
+
+def nvcc() -> str:
+    cand = os.environ.get("NVCC") or "/usr/local/cuda/bin/nvcc"
+    return cand if Path(cand).exists() else "nvcc"
+
+
+def up_to_date() -> bool:
+    if not LIB.exists():
+        return False
+    t = LIB.stat().st_mtime
+    deps = [CSRC / s for s in SOURCES + HEADERS] + [ROOT / "include" / "ses_gpu.h"]
+    return all(d.stat().st_mtime <= t for d in deps)
+
+
+def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
+    if not force and up_to_date():
+        return LIB
+    cmd = [nvcc(), *ARCH, *FLAGS, "-I", str(ROOT / "include"), "-I", str(CSRC)]
+    if ptxas_verbose:
+        cmd += ["-Xptxas", "-v"]
+    cmd += [str(CSRC / s) for s in SOURCES] + ["-o", str(LIB)]
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--verbose-ptxas", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    args = ap.parse_args(argv)
+    print(build(force=args.force or args.verbose_ptxas, ptxas_verbose=args.verbose_ptxas))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

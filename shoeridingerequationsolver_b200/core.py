@@ -1,0 +1,338 @@
+"""Host-side mirror of the reference core's split-operator call surface.
+
+Same names, argument meaning and error behaviour as the reference's C++
+modules (parkyere/ShoeridingerEquationSolver core/src/), backed by the B200
+library through its C ABI:
+
+* ``Grid1D`` / ``Grid3D``          -- core/src/grid.ixx:10-30
+* ``Field1D`` / ``Field3D``        -- core/src/field.ixx:11-66 (numpy complex128 data)
+* ``wavenumbers``                  -- core/src/spectral.ixx:14-23
+* ``fft`` / ``ifft``               -- core/src/fft.ixx:75-188
+* ``SplitOperator3D``              -- core/src/propagator.ixx:68-134, plus the resident
+                                      engine calls of solver/src/vk_engine.ixx
+                                      (upload_state, step(n, absorb), set_absorber,
+                                      readback, norm/energy readouts)
+* ``SplitOperator1D``              -- core/src/propagator.ixx:21-66
+
+Sizes that are not 2^a 3^b 5^c raise ``ValueError`` (the reference raises
+std::invalid_argument for non-powers of two).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, lib
+
+_dp = C.POINTER(C.c_double)
+
+PRECISIONS = {"c128": _abi.SES_C128, "c64": _abi.SES_C64}
+
+
+@dataclass(frozen=True)
+class Grid1D:
+    xmin: float
+    xmax: float
+    n: int
+
+    def size(self) -> int:
+        return self.n
+
+    def spacing(self) -> float:
+        return (self.xmax - self.xmin) / self.n
+
+    def coord(self, i: int) -> float:
+        return self.xmin + i * self.spacing()
+
+    def coords(self) -> np.ndarray:
+        return self.xmin + np.arange(self.n) * self.spacing()
+
+
+@dataclass(frozen=True)
+class Grid3D:
+    x: Grid1D
+    y: Grid1D
+    z: Grid1D
+
+    def size(self) -> int:
+        return self.x.n * self.y.n * self.z.n
+
+    def flat(self, i: int, j: int, k: int) -> int:
+        return i + self.x.n * (j + self.y.n * k)
+
+    def cell_volume(self) -> float:
+        return self.x.spacing() * self.y.spacing() * self.z.spacing()
+
+    @property
+    def shape(self) -> tuple[int, int, int]:
+        """numpy C-order shape (nz, ny, nx) of the x-fastest flat layout."""
+        return (self.z.n, self.y.n, self.x.n)
+
+    @property
+    def box(self) -> tuple[float, ...]:
+        return (self.x.xmin, self.x.xmax, self.y.xmin, self.y.xmax, self.z.xmin, self.z.xmax)
+
+    @property
+    def dims(self) -> tuple[int, int, int]:
+        return (self.x.n, self.y.n, self.z.n)
+
+
+def line_grid(g: Grid1D) -> Grid3D:
+    """A 1D grid as Grid3D (n x 1 x 1) with unit-length collapsed axes."""
+    return Grid3D(g, Grid1D(0.0, 1.0, 1), Grid1D(0.0, 1.0, 1))
+
+
+class Field3D:
+    def __init__(self, grid: Grid3D, data=None):
+        self.grid = grid
+        if data is None:
+            self.data = np.zeros(grid.size(), dtype=np.complex128)
+        else:
+            self.data = np.ascontiguousarray(np.asarray(data, dtype=np.complex128).reshape(-1))
+            if self.data.size != grid.size():
+                raise ValueError("field size does not match the grid")
+
+    def size(self) -> int:
+        return self.grid.size()
+
+    def __call__(self, i: int, j: int, k: int) -> complex:
+        return self.data[self.grid.flat(i, j, k)]
+
+
+class Field1D:
+    def __init__(self, grid: Grid1D, data=None):
+        self.grid = grid
+        self.data = (np.zeros(grid.n, dtype=np.complex128) if data is None else
+                     np.ascontiguousarray(np.asarray(data, dtype=np.complex128).reshape(-1)))
+        if self.data.size != grid.n:
+            raise ValueError("field size does not match the grid")
+
+    def size(self) -> int:
+        return self.grid.n
+
+    def __getitem__(self, i):
+        return self.data[i]
+
+
+def wavenumbers(g: Grid1D) -> np.ndarray:
+    """fftfreq layout: k_j = (2 pi/L) * (j if 2j < n else j - n)."""
+    dk = 2.0 * math.pi / (g.xmax - g.xmin)
+    j = np.arange(g.n)
+    return dk * np.where(2 * j < g.n, j, j - g.n).astype(np.float64)
+
+
+def norm_sq(f) -> float:
+    """sum |psi|^2 times the cell volume (field.ixx:30-36, 68-74)."""
+    if isinstance(f, Field1D):
+        return float(np.sum(np.abs(f.data) ** 2) * f.grid.spacing())
+    return float(np.sum(np.abs(f.data) ** 2) * f.grid.cell_volume())
+
+
+def _fft_host(data: np.ndarray, dims, inverse: bool, precision: str) -> None:
+    n = (C.c_int32 * 3)(*dims)
+    check(lib.ses_fft3_host(n, PRECISIONS[precision], data.ctypes.data_as(_dp), 1 if inverse else 0))
+
+
+def _transform(x, inverse: bool, precision: str):
+    if isinstance(x, Field3D):
+        _fft_host(x.data, x.grid.dims, inverse, precision)
+        return x
+    if isinstance(x, Field1D):
+        _fft_host(x.data, (x.grid.n, 1, 1), inverse, precision)
+        return x
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.complex128))
+    if a.ndim == 1:
+        dims = (a.size, 1, 1)
+    elif a.ndim == 3:
+        dims = (a.shape[2], a.shape[1], a.shape[0])
+    else:
+        raise ValueError("expected a 1D line or a (nz, ny, nx) array")
+    out = a.copy()
+    _fft_host(out.reshape(-1), dims, inverse, precision)
+    return out
+
+
+def fft(x, precision: str = "c128"):
+    """Forward unnormalised FFT (fft.ixx:14-18): Field3D/Field1D in place, arrays by copy."""
+    return _transform(x, False, precision)
+
+
+def ifft(x, precision: str = "c128"):
+    """Inverse FFT with 1/N (fft.ixx:89-98, 177-188)."""
+    return _transform(x, True, precision)
+
+
+class SplitOperator3D:
+    """Strang split-operator propagator on the B200 (propagator.ixx:68-134).
+
+    ``step(psi, nsteps)`` keeps the reference's in-place semantics on a
+    caller-owned Field3D (upload, nsteps Strang steps, readback).  The
+    engine-style calls (``upload_state`` / ``advance`` / ``readback`` /
+    ``observe``) keep psi resident in HBM between calls.
+    """
+
+    def __init__(self, grid: Grid3D, potential, dt: float, mass: float = 1.0,
+                 precision: str = "c128", psi0=None):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {list(PRECISIONS)}")
+        self.grid = grid
+        self.precision = precision
+        self.mass = mass
+        self._dt = float(dt)
+        v = np.ascontiguousarray(np.asarray(potential, dtype=np.float64).reshape(-1))
+        if v.size != grid.size():
+            raise ValueError("potential size does not match the grid")
+        p0 = None
+        if psi0 is not None:
+            p0 = np.ascontiguousarray(np.asarray(psi0, dtype=np.complex128).reshape(-1))
+            if p0.size != grid.size():
+                raise ValueError("psi0 size does not match the grid")
+        h = C.c_void_p()
+        desc = _abi.grid_desc(grid)
+        check(lib.ses_gpu_create(C.byref(desc), PRECISIONS[precision], self._dt, float(mass),
+                                 v.ctypes.data_as(_dp),
+                                 p0.ctypes.data_as(_dp) if p0 is not None else None, C.byref(h)))
+        self._h = h
+
+    # ---- reference surface ----
+    def dt(self) -> float:
+        return self._dt
+
+    def half_potential_phase(self) -> np.ndarray:
+        out = np.empty(self.grid.size(), dtype=np.complex128)
+        check(lib.ses_gpu_tables(self._h, out.ctypes.data_as(_dp), None))
+        return out
+
+    def kinetic_phase(self) -> np.ndarray:
+        out = np.empty(self.grid.size(), dtype=np.complex128)
+        check(lib.ses_gpu_tables(self._h, None, out.ctypes.data_as(_dp)))
+        return out
+
+    def step(self, psi: Field3D, nsteps: int = 1) -> None:
+        if psi.data.size != self.grid.size():
+            raise ValueError("field size does not match the propagator")
+        self.upload_state(psi.data)
+        self.advance(nsteps)
+        self.readback(out=psi.data)
+
+    # ---- resident engine surface ----
+    @property
+    def handle(self):
+        return self._h
+
+    def upload_state(self, psi) -> None:
+        a = np.ascontiguousarray(np.asarray(psi, dtype=np.complex128).reshape(-1))
+        if a.size != self.grid.size():
+            raise ValueError("psi size does not match the grid")
+        check(lib.ses_gpu_write_psi(self._h, a.ctypes.data))
+
+    def write_ptr(self, host_ptr: int) -> None:
+        """Upload from a raw host pointer to N interleaved complex128 values."""
+        check(lib.ses_gpu_write_psi(self._h, C.c_void_p(host_ptr)))
+
+    def read_ptr(self, host_ptr: int) -> None:
+        check(lib.ses_gpu_read_psi(self._h, C.c_void_p(host_ptr)))
+
+    def readback(self, out=None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.grid.size(), dtype=np.complex128)
+        if not (out.flags.c_contiguous and out.dtype == np.complex128 and out.size == self.grid.size()):
+            raise ValueError("readback target must be a contiguous complex128 array of N elements")
+        check(lib.ses_gpu_read_psi(self._h, out.ctypes.data))
+        return out
+
+    def advance(self, nsteps: int, absorb: bool = False) -> None:
+        check(lib.ses_gpu_step(self._h, int(nsteps), 1 if absorb else 0))
+
+    def set_absorber(self, mask) -> None:
+        if mask is None:
+            check(lib.ses_gpu_set_absorber(self._h, None))
+            return
+        m = np.ascontiguousarray(np.asarray(mask, dtype=np.float64).reshape(-1))
+        if m.size != self.grid.size():
+            raise ValueError("mask size does not match the grid")
+        check(lib.ses_gpu_set_absorber(self._h, m.ctypes.data_as(_dp)))
+
+    def set_absorber_separable(self, mx, my, mz) -> None:
+        arrs = [np.ascontiguousarray(np.asarray(a, dtype=np.float64)) for a in (mx, my, mz)]
+        for a, n in zip(arrs, self.grid.dims):
+            if a.size != n:
+                raise ValueError("mask profile size does not match its axis")
+        check(lib.ses_gpu_set_absorber_separable(self._h, *[a.ctypes.data_as(_dp) for a in arrs]))
+
+    def set_potential(self, potential) -> None:
+        v = np.ascontiguousarray(np.asarray(potential, dtype=np.float64).reshape(-1))
+        if v.size != self.grid.size():
+            raise ValueError("potential size does not match the grid")
+        check(lib.ses_gpu_set_potential(self._h, v.ctypes.data_as(_dp)))
+
+    def fft3(self, inverse: bool = False) -> None:
+        check(lib.ses_gpu_fft3(self._h, 1 if inverse else 0))
+
+    def observe(self, xlo: float = -math.inf, xhi: float = math.inf) -> dict:
+        o = _abi.Observables()
+        check(lib.ses_gpu_observe(self._h, float(xlo), float(xhi), C.byref(o)))
+        return o.as_dict()
+
+    def sync(self, timeout_ms: int = 0) -> None:
+        check(lib.ses_gpu_sync(self._h, int(timeout_ms)))
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(lib.ses_gpu_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def psi_device(self) -> tuple[int, int]:
+        p, b = C.c_void_p(), C.c_size_t()
+        check(lib.ses_gpu_psi_device(self._h, C.byref(p), C.byref(b)))
+        return p.value, b.value
+
+    def footprint(self) -> int:
+        b = C.c_size_t()
+        check(lib.ses_gpu_footprint(self._h, C.byref(b)))
+        return b.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(lib.ses_gpu_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class SplitOperator1D:
+    """1D Strang propagator (propagator.ixx:21-66): the 3D engine on n x 1 x 1."""
+
+    def __init__(self, grid: Grid1D, potential, dt: float, precision: str = "c128"):
+        self.grid = grid
+        self._op = SplitOperator3D(line_grid(grid), potential, dt, 1.0, precision)
+
+    def dt(self) -> float:
+        return self._op.dt()
+
+    def step(self, psi: Field1D, nsteps: int = 1) -> None:
+        if psi.data.size != self.grid.n:
+            raise ValueError("field size does not match the propagator")
+        self._op.upload_state(psi.data)
+        self._op.advance(nsteps)
+        self._op.readback(out=psi.data)
+
+    @property
+    def engine(self) -> SplitOperator3D:
+        return self._op
+
+    def close(self) -> None:
+        self._op.close()

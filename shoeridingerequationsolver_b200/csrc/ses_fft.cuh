@@ -1,0 +1,328 @@
+// Device building blocks of the split-operator step: complex arithmetic,
+// in-register radix-2/3/4/5/8/16 DFTs, and one Stockham autosort stage over a
+// tile of L lines held in shared memory.
+//
+// The line FFT is the forward unnormalised transform X_k = sum_n x_n e^{-2 pi i kn/N}
+// of the reference (core/src/fft.ixx:14-18).  Inverse transforms use the
+// conjugation identity ifft(X) = conj(fft(conj(X)))/N (fft.ixx:89-98), with the
+// conjugations and 1/N folded into the neighbouring element-wise operations.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sesk {
+
+constexpr int kMaxStages = 12;
+
+template <typename T>
+struct __align__(2 * sizeof(T)) cx {
+    T x, y;
+};
+
+template <typename T>
+__host__ __device__ __forceinline__ cx<T> mk(T a, T b) {
+    cx<T> r;
+    r.x = a;
+    r.y = b;
+    return r;
+}
+template <typename T>
+__device__ __forceinline__ cx<T> operator+(cx<T> a, cx<T> b) {
+    return mk<T>(a.x + b.x, a.y + b.y);
+}
+template <typename T>
+__device__ __forceinline__ cx<T> operator-(cx<T> a, cx<T> b) {
+    return mk<T>(a.x - b.x, a.y - b.y);
+}
+template <typename T>
+__device__ __forceinline__ cx<T> operator*(cx<T> a, cx<T> b) {
+    return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename T>
+__device__ __forceinline__ cx<T> scale(cx<T> a, T s) {
+    return mk<T>(a.x * s, a.y * s);
+}
+// a * (-i)
+template <typename T>
+__device__ __forceinline__ cx<T> mul_mi(cx<T> a) {
+    return mk<T>(a.y, -a.x);
+}
+template <typename T>
+__device__ __forceinline__ cx<T> cconj(cx<T> a) {
+    return mk<T>(a.x, -a.y);
+}
+template <typename T>
+__device__ __forceinline__ cx<double> widen(cx<T> a) {
+    return mk<double>((double)a.x, (double)a.y);
+}
+template <typename T>
+__device__ __forceinline__ cx<T> narrow(cx<double> a) {
+    return mk<T>((T)a.x, (T)a.y);
+}
+
+// Division by a run-time invariant divisor with one multiply-high and a shift
+// (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994).  Valid for dividends below 2^31.
+struct FastDiv {
+    uint32_t d, mul, shr;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+    FastDiv f{d, 0u, 0u};
+    if (d <= 1) return f;
+    uint32_t l = 0;
+    while ((1ull << l) < d) ++l;            // ceil(log2 d)
+    const uint32_t p = 31 + l;
+    f.mul = (uint32_t)(((1ull << p) + d - 1) / d);
+    f.shr = p - 32;
+    return f;
+}
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t x, const FastDiv& f) {
+    return f.d <= 1 ? x : (__umulhi(x, f.mul) >> f.shr);
+}
+
+// ---------------------------------------------------------------------------
+// In-register DFTs of size R, forward (e^{-}), natural-order output.
+// The constants are cos/sin of the R-th roots of unity.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void dft2(cx<T>* v) {
+    const cx<T> a = v[0];
+    v[0] = a + v[1];
+    v[1] = a - v[1];
+}
+
+template <typename T>
+__device__ __forceinline__ void dft4(cx<T>* v) {
+    const cx<T> t0 = v[0] + v[2], t1 = v[0] - v[2];
+    const cx<T> t2 = v[1] + v[3], t3 = mul_mi(v[1] - v[3]);
+    v[0] = t0 + t2;
+    v[2] = t0 - t2;
+    v[1] = t1 + t3;
+    v[3] = t1 - t3;
+}
+
+template <typename T>
+__device__ __forceinline__ void dft8(cx<T>* v) {
+    const T h = (T)0.70710678118654752440;
+    cx<T> e[4] = {v[0], v[2], v[4], v[6]};
+    cx<T> o[4] = {v[1], v[3], v[5], v[7]};
+    dft4(e);
+    dft4(o);
+    o[1] = mk<T>((o[1].x + o[1].y) * h, (o[1].y - o[1].x) * h);   // * e^{-i pi/4}
+    o[2] = mul_mi(o[2]);                                          // * e^{-i pi/2}
+    o[3] = mk<T>((o[3].y - o[3].x) * h, -(o[3].x + o[3].y) * h);  // * e^{-3i pi/4}
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        v[k] = e[k] + o[k];
+        v[k + 4] = e[k] - o[k];
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void dft16(cx<T>* v) {
+    const T c1 = (T)0.92387953251128675613;  // cos(pi/8)
+    const T s1 = (T)0.38268343236508977173;  // sin(pi/8)
+    const T h = (T)0.70710678118654752440;   // cos(pi/4)
+    cx<T> e[8], o[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        e[k] = v[2 * k];
+        o[k] = v[2 * k + 1];
+    }
+    dft8(e);
+    dft8(o);
+    // o[k] *= e^{-2 pi i k / 16}
+    o[1] = o[1] * mk<T>(c1, -s1);
+    o[2] = mk<T>((o[2].x + o[2].y) * h, (o[2].y - o[2].x) * h);
+    o[3] = o[3] * mk<T>(s1, -c1);
+    o[4] = mul_mi(o[4]);
+    o[5] = o[5] * mk<T>(-s1, -c1);
+    o[6] = mk<T>((o[6].y - o[6].x) * h, -(o[6].x + o[6].y) * h);
+    o[7] = o[7] * mk<T>(-c1, -s1);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        v[k] = e[k] + o[k];
+        v[k + 8] = e[k] - o[k];
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void dft3(cx<T>* v) {
+    const T hs3 = (T)0.86602540378443864676;  // sin(2 pi/3)
+    const cx<T> t = v[1] + v[2];
+    const cx<T> m = mk<T>(v[0].x - (T)0.5 * t.x, v[0].y - (T)0.5 * t.y);
+    const cx<T> d = scale(v[1] - v[2], hs3);
+    v[0] = v[0] + t;
+    v[1] = mk<T>(m.x + d.y, m.y - d.x);  // m - i d
+    v[2] = mk<T>(m.x - d.y, m.y + d.x);  // m + i d
+}
+
+template <typename T>
+__device__ __forceinline__ void dft5(cx<T>* v) {
+    const T c1 = (T)0.30901699437494742410;   // cos(2 pi/5)
+    const T c2 = (T)-0.80901699437494742410;  // cos(4 pi/5)
+    const T s1 = (T)0.95105651629515357212;   // sin(2 pi/5)
+    const T s2 = (T)0.58778525229247312917;   // sin(4 pi/5)
+    const cx<T> a1 = v[1] + v[4], a2 = v[2] + v[3];
+    const cx<T> b1 = v[1] - v[4], b2 = v[2] - v[3];
+    const cx<T> p1 = mk<T>(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
+    const cx<T> p2 = mk<T>(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
+    const cx<T> q1 = mk<T>(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y);
+    const cx<T> q2 = mk<T>(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y);
+    v[0] = v[0] + a1 + a2;
+    v[1] = mk<T>(p1.x + q1.y, p1.y - q1.x);  // p1 - i q1
+    v[4] = mk<T>(p1.x - q1.y, p1.y + q1.x);  // p1 + i q1
+    v[2] = mk<T>(p2.x + q2.y, p2.y - q2.x);
+    v[3] = mk<T>(p2.x - q2.y, p2.y + q2.x);
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void dft(cx<T>* v) {
+    if constexpr (R == 2) dft2(v);
+    else if constexpr (R == 3) dft3(v);
+    else if constexpr (R == 4) dft4(v);
+    else if constexpr (R == 5) dft5(v);
+    else if constexpr (R == 8) dft8(v);
+    else if constexpr (R == 16) dft16(v);
+}
+
+// ---------------------------------------------------------------------------
+// Geometry of one axis pass.  A CTA owns a tile of L lines (L a power of two)
+// of one axis of length n.  Shared-memory address of element e of tile line l
+// is l*ls + e*es: (ls, es) = (pitch, 1) for contiguous-axis tiles, (1, L) for
+// strided-axis tiles.  Butterflies are numbered line-fastest (b -> l = b % L,
+// j = b / L) so consecutive threads touch consecutive lines: conflict-free in
+// both layouts (the contiguous layout pads its pitch to an odd length).
+// ---------------------------------------------------------------------------
+struct Geo {
+    int n;         // axis length
+    int L;         // lines per tile
+    int lshift;    // log2(L)
+    int nthreads;  // threads per CTA
+    int ls, es;    // shared-memory strides
+    int nst;       // Stockham stages
+    int rad[kMaxStages];
+    int Ns[kMaxStages];        // product of the previous radices
+    int twstride[kMaxStages];  // n / (Ns * R)
+    FastDiv fNs[kMaxStages];
+    FastDiv fn;                // division by n
+};
+
+// One Stockham autosort stage of radix R (E. Bainville's formulation of the
+// mixed-radix Stockham FFT): butterfly j of span Ns reads x[j + r n/R],
+// applies twiddles w^{r k n/(Ns R)} (k = j mod Ns) and writes
+// y[(j - k) R + k + r Ns].
+//
+// STREAM: source and destination are different memories (HBM -> tile or
+// tile -> HBM), so each thread runs its butterflies start to finish.
+// Otherwise the stage is in place in the tile: a thread reads all of its (up
+// to B) butterflies into registers, the CTA synchronises, then writes.
+template <typename T, int R, int B, bool STREAM, class LD, class ST>
+__device__ __forceinline__ void stage(const Geo& g, int p, const cx<T>* __restrict__ tw, LD& ld,
+                                      ST& st) {
+    const int n = g.n;
+    const int nR = n / R;
+    const int nb = g.L * nR;
+    const int Ns = g.Ns[p];
+    const int tws = g.twstride[p];
+    const FastDiv fNs = g.fNs[p];
+    if constexpr (STREAM) {
+        for (int b = (int)threadIdx.x; b < nb; b += g.nthreads) {
+            const int l = b & (g.L - 1), j = b >> g.lshift;
+            cx<T> v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = ld(l, j + r * nR);
+            const int k = j - (int)fdiv((uint32_t)j, fNs) * Ns;
+            if (Ns > 1) {
+                const int t1 = k * tws;
+#pragma unroll
+                for (int r = 1; r < R; ++r) v[r] = v[r] * tw[r * t1];
+            }
+            dft<T, R>(v);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) st(l, base + r * Ns, v[r]);
+        }
+    } else {
+        cx<T> v[B > 0 ? B : 1][R];
+#pragma unroll
+        for (int it = 0; it < B; ++it) {
+            const int b = (int)threadIdx.x + it * g.nthreads;
+            if (b < nb) {
+                const int l = b & (g.L - 1), j = b >> g.lshift;
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[it][r] = ld(l, j + r * nR);
+                if (Ns > 1) {
+                    const int k = j - (int)fdiv((uint32_t)j, fNs) * Ns;
+                    const int t1 = k * tws;
+#pragma unroll
+                    for (int r = 1; r < R; ++r) v[it][r] = v[it][r] * tw[r * t1];
+                }
+                dft<T, R>(v[it]);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < B; ++it) {
+            const int b = (int)threadIdx.x + it * g.nthreads;
+            if (b < nb) {
+                const int l = b & (g.L - 1), j = b >> g.lshift;
+                const int k = j - (int)fdiv((uint32_t)j, fNs) * Ns;
+                const int base = (j - k) * R + k;
+#pragma unroll
+                for (int r = 0; r < R; ++r) st(l, base + r * Ns, v[it][r]);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, int EPT, int R, class LD, class ST>
+__device__ __forceinline__ void stage_any(const Geo& g, int p, bool stream, const cx<T>* tw, LD& ld,
+                                          ST& st) {
+    if (stream) stage<T, R, EPT / R, true>(g, p, tw, ld, st);
+    else stage<T, R, EPT / R, false>(g, p, tw, ld, st);
+}
+
+// Full line FFT over the tile: stage 0 reads through ld0 (HBM when G_IN, the
+// tile otherwise, with any element-wise pre-op), the last stage writes through
+// stn (HBM when G_OUT, the tile otherwise, with any post-op); intermediate
+// stages stay in the shared tile.  EPT bounds the elements a thread holds in
+// an in-place stage (B = EPT / R butterflies).
+template <typename T, int EPT, bool G_IN, bool G_OUT, class LD0, class STN>
+__device__ __forceinline__ void fft_tile(const Geo& g, cx<T>* sm, const cx<T>* __restrict__ tw,
+                                         LD0& ld0, STN& stn) {
+    if (g.nst == 0) {  // length-1 axis: identity transform, element ops still apply
+        for (int l = threadIdx.x; l < g.L; l += g.nthreads) stn(l, 0, ld0(l, 0));
+        __syncthreads();
+        return;
+    }
+    for (int p = 0; p < g.nst; ++p) {
+        const bool first = p == 0, last = p == g.nst - 1;
+        // stream only when the stage's source and destination cannot alias
+        const bool stream = (first && G_IN && !last) || (last && G_OUT && !first);
+        auto ld = [&](int l, int e) -> cx<T> {
+            return first ? ld0(l, e) : sm[l * g.ls + e * g.es];
+        };
+        auto st = [&](int l, int e, cx<T> v) {
+            if (last) stn(l, e, v);
+            else sm[l * g.ls + e * g.es] = v;
+        };
+        switch (g.rad[p]) {
+            case 2: stage_any<T, EPT, 2>(g, p, stream, tw, ld, st); break;
+            case 3: stage_any<T, EPT, 3>(g, p, stream, tw, ld, st); break;
+            case 4: stage_any<T, EPT, 4>(g, p, stream, tw, ld, st); break;
+            case 5: stage_any<T, EPT, 5>(g, p, stream, tw, ld, st); break;
+            case 8: stage_any<T, EPT, 8>(g, p, stream, tw, ld, st); break;
+            case 16:
+                if constexpr (EPT >= 16) stage_any<T, EPT, 16>(g, p, stream, tw, ld, st);
+                break;
+            default: break;
+        }
+    }
+}
+
+}  // namespace sesk

@@ -1,0 +1,910 @@
+// Host side of the C ABI declared in include/ses_gpu.h: axis plans, the
+// solver handle (resident psi + FP64-built tables in HBM), the Strang step
+// program, observables and the fft / tables surfaces.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "ses_gpu.h"
+#include "ses_pass.cuh"
+
+using namespace sesk;
+
+namespace {
+
+thread_local std::string g_err;
+
+ses_status fail(ses_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+
+#define SES_CU(call)                                                                            \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return fail(SES_EDEVICE, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+    } while (0)
+
+#define SES_TRY(expr)                  \
+    do {                               \
+        ses_status s_ = (expr);        \
+        if (s_ != SES_OK) return s_;   \
+    } while (0)
+
+constexpr int kEPT = kEPTDev;      // elements a thread holds per in-place Stockham stage
+constexpr int kMaxLog2Radix = kEPTDev >= 16 ? 4 : 3;
+constexpr int kMaxAxis = 4096;    // longest supported axis
+constexpr int kObsBlocks = 592;   // 4 x 148 SMs, fixed -> deterministic sums
+constexpr int kBodyUnroll = 8;    // interior steps per captured graph launch
+
+bool factor_radices(int n, std::vector<int>& rad) {
+    rad.clear();
+    if (n < 1) return false;
+    int a = 0, b = 0, c = 0, m = n;
+    while (m % 2 == 0) { m /= 2; ++a; }
+    while (m % 3 == 0) { m /= 3; ++b; }
+    while (m % 5 == 0) { m /= 5; ++c; }
+    if (m != 1) return false;
+    if (a) {  // power-of-two part: fewest radix <= kMaxRadix stages, exponents balanced
+        const int p = (a + kMaxLog2Radix - 1) / kMaxLog2Radix, base = a / p, extra = a % p;
+        for (int i = 0; i < p; ++i) rad.push_back(1 << (base + (i < extra ? 1 : 0)));
+    }
+    for (int i = 0; i < b; ++i) rad.push_back(3);
+    for (int i = 0; i < c; ++i) rad.push_back(5);
+    return true;
+}
+
+struct PassPlan {
+    Geo g{};
+    size_t smem = 0;
+    unsigned grid = 0;
+    long long nlines = 0;
+    long long nu = 0, sw = 0, se = 0;
+};
+
+int threads_for(int L, int n, const std::vector<int>& rad) {
+    int t = 32;
+    for (int R : rad) {
+        const int B = kEPT / R;
+        const long long nb = (long long)L * n / R;
+        t = std::max<long long>(t, (nb + B - 1) / B);
+    }
+    return (t + 31) / 32 * 32;
+}
+
+// Tile shape of one axis pass: L lines of length n, rows of >= 128/256 B for
+// coalescing, tile <= 64 KB of shared memory, <= 512 threads.
+bool plan_pass(int n, int esize, bool strided, long long nlines, PassPlan& pp, std::string& why) {
+    std::vector<int> rad;
+    if (!factor_radices(n, rad)) {
+        why = "axis length " + std::to_string(n) + " is not of the form 2^a 3^b 5^c";
+        return false;
+    }
+    if (n > kMaxAxis) {
+        why = "axis length " + std::to_string(n) + " exceeds " + std::to_string(kMaxAxis);
+        return false;
+    }
+    int L = strided ? 256 / esize : 128 / esize;
+    while ((long long)L * n < 2048 && L < 256) L *= 2;
+    const int pitch = strided ? n : (n % 2 == 0 ? n + 1 : n);
+    while (L > 1 && (size_t)L * pitch * esize > 64 * 1024) L /= 2;
+    while (L > 1 && L / 2 >= nlines) L /= 2;
+    int T = threads_for(L, n, rad);
+    while (T > 512 && L > 1) {
+        L /= 2;
+        T = threads_for(L, n, rad);
+    }
+    if (T > 512) {
+        why = "no tile shape for axis length " + std::to_string(n);
+        return false;
+    }
+    Geo& g = pp.g;
+    g = Geo{};
+    g.n = n;
+    g.L = L;
+    g.lshift = 0;
+    while ((1 << g.lshift) < L) ++g.lshift;
+    g.nthreads = T;
+    g.ls = strided ? 1 : pitch;
+    g.es = strided ? L : 1;
+    g.nst = (int)rad.size();
+    int Ns = 1;
+    for (int p = 0; p < g.nst; ++p) {
+        g.rad[p] = rad[p];
+        g.Ns[p] = Ns;
+        g.twstride[p] = n / (Ns * rad[p]);
+        g.fNs[p] = make_fastdiv((uint32_t)Ns);
+        Ns *= rad[p];
+    }
+    g.fn = make_fastdiv((uint32_t)n);
+    pp.nlines = nlines;
+    pp.grid = (unsigned)((nlines + L - 1) / L);
+    pp.smem = (size_t)L * pitch * esize;
+    if (strided) pp.smem = ((pp.smem + 15) & ~(size_t)15) + (size_t)L * (16 + 16 + 8);
+    return true;
+}
+
+}  // namespace
+
+struct ses_solver {
+    int dev = 0;
+    ses_precision prec = SES_C128;
+    int esize = 16;
+    double box[6] = {0, 1, 0, 1, 0, 1};
+    int n[3] = {1, 1, 1};
+    long long N = 0;
+    double dt = 0.0, mass = 1.0;
+    bool with_tables = true;
+
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaStream_t cap = nullptr;  // private capture stream for graphs
+    cudaEvent_t ev = nullptr;
+
+    void* psi = nullptr;
+    void* scratch = nullptr;
+    void* vtab = nullptr;
+    double* V = nullptr;
+    void* tw[3] = {nullptr, nullptr, nullptr};
+    double* kv[3] = {nullptr, nullptr, nullptr};
+    cx<double>* kd[3] = {nullptr, nullptr, nullptr};
+    double* mask1[3] = {nullptr, nullptr, nullptr};
+    double* maskfull = nullptr;
+    bool has_mask = false;
+
+    PassPlan pp[3];
+    int last_axis = 0;  // highest axis with n > 1 (0 for 1D / single point)
+
+    double* partials = nullptr;
+    size_t partial_rows = 0;
+    double* dsums = nullptr;
+    double* hsums = nullptr;  // pinned
+
+    cudaGraphExec_t body[2] = {nullptr, nullptr};
+    size_t bytes = 0;
+};
+
+namespace {
+
+ses_status dalloc(ses_solver* h, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(SES_ENOMEM, "cudaMalloc(" + std::to_string(bytes) + " B) failed: " +
+                                    cudaGetErrorString(e));
+    }
+    h->bytes += bytes;
+    return SES_OK;
+}
+
+void drop_graphs(ses_solver* h) {
+    for (auto& g : h->body) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+void release(ses_solver* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graphs(h);
+    void* ptrs[] = {h->psi, h->scratch, h->vtab, h->V, h->maskfull, h->partials, h->dsums};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (int a = 0; a < 3; ++a) {
+        if (h->tw[a]) cudaFree(h->tw[a]);
+        if (h->kv[a]) cudaFree(h->kv[a]);
+        if (h->kd[a]) cudaFree(h->kd[a]);
+        if (h->mask1[a]) cudaFree(h->mask1[a]);
+    }
+    if (h->hsums) cudaFreeHost(h->hsums);
+    if (h->ev) cudaEventDestroy(h->ev);
+    if (h->cap) cudaStreamDestroy(h->cap);
+    if (h->own) cudaStreamDestroy(h->own);
+    delete h;
+}
+
+template <typename K>
+void set_smem_attr(K kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+// Bounded wait on everything queued so far on the handle's stream.
+ses_status wait_bounded(ses_solver* h, int timeout_ms) {
+    if (timeout_ms <= 0) timeout_ms = 10000;
+    SES_CU(cudaEventRecord(h->ev, h->stream));
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(h->ev);
+        if (q == cudaSuccess) return SES_OK;
+        if (q != cudaErrorNotReady)
+            return fail(SES_EDEVICE, std::string("device error: ") + cudaGetErrorString(q));
+        const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                            std::chrono::steady_clock::now() - t0)
+                            .count();
+        if (ms > timeout_ms)
+            return fail(SES_ETIMEDOUT, "wait exceeded " + std::to_string(timeout_ms) + " ms");
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+template <typename T>
+PassArgs<T> make_args(const ses_solver* h, int axis, const void* src, void* dst) {
+    PassArgs<T> a{};
+    a.src = reinterpret_cast<const cx<T>*>(src);
+    a.dst = reinterpret_cast<cx<T>*>(dst);
+    a.g = h->pp[axis].g;
+    a.axis = axis;
+    a.nx = h->n[0];
+    a.ny = h->n[1];
+    a.nz = h->n[2];
+    a.nlines = h->pp[axis].nlines;
+    const long long nx = h->n[0], ny = h->n[1];
+    if (axis == 0) {
+        a.nu = a.nlines;
+        a.sw = 0;
+        a.se = 1;
+    } else if (axis == 1) {
+        a.nu = nx;
+        a.sw = nx * ny;
+        a.se = nx;
+    } else {
+        a.nu = nx * ny;
+        a.sw = 0;
+        a.se = nx * ny;
+    }
+    a.fnu = make_fastdiv((uint32_t)a.nu);
+    a.fny = make_fastdiv((uint32_t)ny);
+    a.fnx = make_fastdiv((uint32_t)nx);
+    a.tw = reinterpret_cast<const cx<T>*>(h->tw[axis]);
+    a.out_scale = 1.0;
+    Tables& tb = a.tb;
+    tb.vtab = h->vtab;
+    for (int q = 0; q < 3; ++q) {
+        tb.mask1[q] = h->mask1[q];
+        tb.kd[q] = h->kd[q];
+        tb.kv[q] = h->kv[q];
+    }
+    tb.maskfull = h->maskfull;
+    tb.inv_mass = 1.0 / h->mass;
+    tb.kscale = 1.0 / (double)h->N;
+    a.partials = h->partials;
+    return a;
+}
+
+template <typename T>
+using XKernel = void (*)(const PassArgs<T>);
+
+template <typename T>
+XKernel<T> xkernel(int mode) {
+    switch (mode) {
+        case XM_FWD: return xpass_kernel<T, XM_FWD>;
+        case XM_INV: return xpass_kernel<T, XM_INV>;
+        case XM_START: return xpass_kernel<T, XM_START>;
+        case XM_MID: return xpass_kernel<T, XM_MID>;
+        case XM_END: return xpass_kernel<T, XM_END>;
+        case XM_1D: return xpass_kernel<T, XM_1D>;
+        default: return xpass_kernel<T, XM_REDUCE>;
+    }
+}
+
+template <typename T>
+XKernel<T> skernel(int mode) {
+    switch (mode) {
+        case SM_FWD: return spass_kernel<T, SM_FWD>;
+        case SM_INV: return spass_kernel<T, SM_INV>;
+        case SM_FUSED: return spass_kernel<T, SM_FUSED>;
+        default: return spass_kernel<T, SM_REDUCE>;
+    }
+}
+
+template <typename T>
+ses_status launch(const ses_solver* h, int axis, int mode, const PassArgs<T>& a, cudaStream_t s) {
+    const PassPlan& pp = h->pp[axis];
+    XKernel<T> k = axis == 0 ? xkernel<T>(mode) : skernel<T>(mode);
+    k<<<pp.grid, pp.g.nthreads, pp.smem, s>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(SES_EDEVICE, std::string("pass launch: ") + cudaGetErrorString(e));
+    return SES_OK;
+}
+
+struct XProg {
+    int mode = XM_FWD;
+    int d_load = DG_NONE, d_mid = DG_NONE, d_store = DG_NONE;
+    int m_load = 0, m_mid = 0, m_store = 0;
+    double out_scale = 1.0;
+};
+
+template <typename T>
+ses_status pass_x(const ses_solver* h, const void* src, void* dst, const XProg& p, cudaStream_t s) {
+    PassArgs<T> a = make_args<T>(h, 0, src, dst);
+    a.d_load = p.d_load;
+    a.d_mid = p.d_mid;
+    a.d_store = p.d_store;
+    a.m_load = p.m_load;
+    a.m_mid = p.m_mid;
+    a.m_store = p.m_store;
+    a.out_scale = p.out_scale;
+    return launch<T>(h, 0, p.mode, a, s);
+}
+
+template <typename T>
+ses_status pass_s(const ses_solver* h, int axis, const void* src, void* dst, int mode, double scale_,
+                  cudaStream_t s) {
+    PassArgs<T> a = make_args<T>(h, axis, src, dst);
+    a.out_scale = scale_;
+    return launch<T>(h, axis, mode, a, s);
+}
+
+template <typename T>
+void set_attrs_prec() {
+    for (int m = XM_FWD; m <= XM_REDUCE; ++m) set_smem_attr(xkernel<T>(m));
+    for (int m = SM_FWD; m <= SM_REDUCE; ++m) set_smem_attr(skernel<T>(m));
+}
+
+void init_kernel_attrs() {
+    static bool done = false;
+    if (done) return;
+    set_attrs_prec<float>();
+    set_attrs_prec<double>();
+    done = true;
+}
+
+// y/z part of one step: fwd y, fused z, inv y (3D) or fused y (2D) or fused z.
+template <typename T>
+ses_status mid_axes(const ses_solver* h, cudaStream_t s) {
+    if (h->last_axis == 2) {
+        if (h->n[1] > 1) SES_TRY(pass_s<T>(h, 1, h->psi, h->psi, SM_FWD, 1.0, s));
+        SES_TRY(pass_s<T>(h, 2, h->psi, h->psi, SM_FUSED, 1.0, s));
+        if (h->n[1] > 1) SES_TRY(pass_s<T>(h, 1, h->psi, h->psi, SM_INV, 1.0, s));
+    } else if (h->last_axis == 1) {
+        SES_TRY(pass_s<T>(h, 1, h->psi, h->psi, SM_FUSED, 1.0, s));
+    }
+    return SES_OK;
+}
+
+// One interior unit of the merged Strang batch.
+template <typename T>
+ses_status interior_unit(const ses_solver* h, bool mask, cudaStream_t s) {
+    XProg p;
+    if (h->last_axis == 0) {  // 1D: [V M, fwd, K/N, inv]
+        p.mode = XM_1D;
+        p.d_load = DG_FULL;
+        p.m_load = mask;
+        return pass_x<T>(h, h->psi, h->psi, p, s);
+    }
+    p.mode = XM_MID;
+    p.d_mid = DG_FULL;
+    p.m_mid = mask;
+    SES_TRY(pass_x<T>(h, h->psi, h->psi, p, s));
+    return mid_axes<T>(h, s);
+}
+
+template <typename T>
+ses_status ensure_body(ses_solver* h, bool mask) {
+    cudaGraphExec_t& ex = h->body[mask ? 1 : 0];
+    if (ex) return SES_OK;
+    if (!h->cap) SES_CU(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
+    SES_CU(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+    ses_status st = SES_OK;
+    for (int u = 0; u < kBodyUnroll && st == SES_OK; ++u) st = interior_unit<T>(h, mask, h->cap);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->cap, &graph);
+    if (st != SES_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (e != cudaSuccess) return fail(SES_EDEVICE, std::string("graph capture: ") + cudaGetErrorString(e));
+    const cudaError_t ie = cudaGraphInstantiate(&ex, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+        ex = nullptr;
+        return fail(SES_EDEVICE, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    return SES_OK;
+}
+
+template <typename T>
+ses_status enqueue_steps(ses_solver* h, int S, bool mask) {
+    cudaStream_t s = h->stream;
+    if (h->last_axis == 0) {
+        // 1D batch: [Vh] U [V M] U ... U [Vh M], each step one fused x pass
+        XProg first;
+        first.mode = XM_1D;
+        first.d_load = DG_HALF;
+        if (S == 1) {
+            first.d_store = DG_HALF;
+            first.m_store = mask;
+        }
+        SES_TRY(pass_x<T>(h, h->psi, h->psi, first, s));
+        if (S == 1) return SES_OK;
+        int interior = S - 2;
+        if (interior >= kBodyUnroll) SES_TRY(ensure_body<T>(h, mask));
+        while (interior >= kBodyUnroll) {
+            SES_CU(cudaGraphLaunch(h->body[mask ? 1 : 0], s));
+            interior -= kBodyUnroll;
+        }
+        for (; interior > 0; --interior) SES_TRY(interior_unit<T>(h, mask, s));
+        XProg lastp;
+        lastp.mode = XM_1D;
+        lastp.d_load = DG_FULL;
+        lastp.m_load = mask;
+        lastp.d_store = DG_HALF;
+        lastp.m_store = mask;
+        return pass_x<T>(h, h->psi, h->psi, lastp, s);
+    }
+    XProg start;
+    start.mode = XM_START;
+    start.d_load = DG_HALF;
+    SES_TRY(pass_x<T>(h, h->psi, h->psi, start, s));
+    SES_TRY(mid_axes<T>(h, s));
+    int interior = S - 1;
+    if (interior >= kBodyUnroll) SES_TRY(ensure_body<T>(h, mask));
+    while (interior >= kBodyUnroll) {
+        SES_CU(cudaGraphLaunch(h->body[mask ? 1 : 0], s));
+        interior -= kBodyUnroll;
+    }
+    for (; interior > 0; --interior) SES_TRY(interior_unit<T>(h, mask, s));
+    XProg end;
+    end.mode = XM_END;
+    end.d_store = DG_HALF;
+    end.m_store = mask;
+    return pass_x<T>(h, h->psi, h->psi, end, s);
+}
+
+template <typename T>
+ses_status enqueue_fft3(ses_solver* h, void* data, int inverse) {
+    cudaStream_t s = h->stream;
+    if (!inverse) {
+        XProg p;
+        p.mode = XM_FWD;
+        SES_TRY(pass_x<T>(h, data, data, p, s));
+        if (h->n[1] > 1) SES_TRY(pass_s<T>(h, 1, data, data, SM_FWD, 1.0, s));
+        if (h->n[2] > 1) SES_TRY(pass_s<T>(h, 2, data, data, SM_FWD, 1.0, s));
+        return SES_OK;
+    }
+    if (h->n[2] > 1) SES_TRY(pass_s<T>(h, 2, data, data, SM_INV, 1.0, s));
+    if (h->n[1] > 1) SES_TRY(pass_s<T>(h, 1, data, data, SM_INV, 1.0, s));
+    XProg p;
+    p.mode = XM_INV;
+    p.out_scale = 1.0 / (double)h->N;
+    return pass_x<T>(h, data, data, p, s);
+}
+
+template <typename T>
+ses_status enqueue_observe(ses_solver* h, double xlo, double xhi) {
+    cudaStream_t s = h->stream;
+    ObsArgs o{};
+    o.N = h->N;
+    o.nx = h->n[0];
+    o.ny = h->n[1];
+    o.fnx = make_fastdiv((uint32_t)h->n[0]);
+    o.fny = make_fastdiv((uint32_t)h->n[1]);
+    o.x0 = h->box[0];
+    o.hx = (h->box[1] - h->box[0]) / h->n[0];
+    o.y0 = h->box[2];
+    o.hy = (h->box[3] - h->box[2]) / h->n[1];
+    o.z0 = h->box[4];
+    o.hz = (h->box[5] - h->box[4]) / h->n[2];
+    o.xlo = xlo;
+    o.xhi = xhi;
+    obs_real_kernel<T><<<kObsBlocks, 256, 0, s>>>(reinterpret_cast<const cx<T>*>(h->psi), h->V, o,
+                                                  h->partials);
+    finalize_kernel<<<1, 32, 0, s>>>(h->partials, kObsBlocks, kRedR, h->dsums);
+    SES_CU(cudaGetLastError());
+    // k-space: phi = FFT(psi) into the scratch field, reduced in the last pass
+    unsigned rows = 0;
+    if (h->last_axis == 0) {
+        XProg p;
+        p.mode = XM_REDUCE;
+        SES_TRY(pass_x<T>(h, h->psi, h->scratch, p, s));
+        rows = h->pp[0].grid;
+    } else {
+        XProg p;
+        p.mode = XM_FWD;
+        SES_TRY(pass_x<T>(h, h->psi, h->scratch, p, s));
+        if (h->last_axis == 2 && h->n[1] > 1)
+            SES_TRY(pass_s<T>(h, 1, h->scratch, h->scratch, SM_FWD, 1.0, s));
+        SES_TRY(pass_s<T>(h, h->last_axis, h->scratch, h->scratch, SM_REDUCE, 1.0, s));
+        rows = h->pp[h->last_axis].grid;
+    }
+    finalize_kernel<<<1, 32, 0, s>>>(h->partials, (int)rows, kRedK, h->dsums + kRedR);
+    SES_CU(cudaGetLastError());
+    SES_CU(cudaMemcpyAsync(h->hsums, h->dsums, (kRedR + kRedK) * sizeof(double),
+                           cudaMemcpyDeviceToHost, s));
+    return SES_OK;
+}
+
+ses_status check_handle(ses_handle h) {
+    if (!h) return fail(SES_EINVAL, "null handle");
+    return SES_OK;
+}
+
+template <typename T>
+ses_status build_tables(ses_solver* h) {
+    const long long N = h->N;
+    const int tb = 256;
+    const unsigned gb = (unsigned)std::min<long long>((N + tb - 1) / tb, 148 * 32);
+    if (h->prec == SES_C128)
+        build_vtab_c128<<<gb, tb, 0, h->stream>>>(h->V, reinterpret_cast<cx<double>*>(h->vtab), N,
+                                                   h->dt);
+    else
+        build_vtab_c64<<<gb, tb, 0, h->stream>>>(h->V, reinterpret_cast<cx<float>*>(h->vtab), N,
+                                                  h->dt);
+    SES_CU(cudaGetLastError());
+    return SES_OK;
+}
+
+ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt, double mass,
+                       const double* V, const double* psi0, bool with_tables, ses_handle* out) {
+    if (!grid || !out) return fail(SES_EINVAL, "null grid or output pointer");
+    *out = nullptr;
+    if (prec != SES_C128 && prec != SES_C64) return fail(SES_EINVAL, "unknown precision");
+    const ses_axis ax[3] = {grid->x, grid->y, grid->z};
+    for (int a = 0; a < 3; ++a) {
+        if (ax[a].n < 1) return fail(SES_EINVAL, "axis length must be >= 1");
+        if (!(ax[a].xmax > ax[a].xmin)) return fail(SES_EINVAL, "axis needs xmax > xmin");
+    }
+    const long long N = (long long)ax[0].n * ax[1].n * ax[2].n;
+    if (N >= (1ll << 31)) return fail(SES_EINVAL, "grid exceeds 2^31 points");
+    if (with_tables) {
+        if (!V) return fail(SES_EINVAL, "potential pointer is null");
+        if (!(mass > 0.0)) return fail(SES_EINVAL, "mass must be > 0");
+        if (!std::isfinite(dt)) return fail(SES_EINVAL, "dt must be finite");
+    }
+    init_kernel_attrs();
+
+    ses_solver* h = new ses_solver();
+    h->prec = prec;
+    h->esize = prec == SES_C128 ? 16 : 8;
+    h->N = N;
+    h->dt = dt;
+    h->mass = mass;
+    h->with_tables = with_tables;
+    for (int a = 0; a < 3; ++a) {
+        h->n[a] = ax[a].n;
+        h->box[2 * a] = ax[a].xmin;
+        h->box[2 * a + 1] = ax[a].xmax;
+    }
+    cudaGetDevice(&h->dev);
+    h->last_axis = h->n[2] > 1 ? 2 : (h->n[1] > 1 ? 1 : 0);
+
+    auto bail = [&](ses_status s) {
+        release(h);
+        return s;
+    };
+    const long long nlines[3] = {(long long)h->n[1] * h->n[2], (long long)h->n[0] * h->n[2],
+                                 (long long)h->n[0] * h->n[1]};
+    size_t rows = kObsBlocks;
+    for (int a = 0; a < 3; ++a) {
+        std::string why;
+        if (!plan_pass(h->n[a], h->esize, a != 0, nlines[a], h->pp[a], why))
+            return bail(fail(SES_EINVAL, why));
+        rows = std::max<size_t>(rows, h->pp[a].grid);
+    }
+    if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(fail(SES_EDEVICE, "stream/event creation failed"));
+    }
+    h->stream = h->own;
+
+    ses_status st;
+    if ((st = dalloc(h, &h->psi, N * h->esize)) != SES_OK) return bail(st);
+    if ((st = dalloc(h, &h->scratch, N * h->esize)) != SES_OK) return bail(st);
+    h->partial_rows = rows;
+    if ((st = dalloc(h, (void**)&h->partials, rows * kRedR * sizeof(double))) != SES_OK) return bail(st);
+    if ((st = dalloc(h, (void**)&h->dsums, 32 * sizeof(double))) != SES_OK) return bail(st);
+    if (cudaMallocHost((void**)&h->hsums, 32 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(fail(SES_ENOMEM, "pinned host allocation failed"));
+    }
+    for (int a = 0; a < 3; ++a) {
+        const int n = h->n[a];
+        if ((st = dalloc(h, &h->tw[a], (size_t)n * h->esize)) != SES_OK) return bail(st);
+        if ((st = dalloc(h, (void**)&h->kv[a], (size_t)n * sizeof(double))) != SES_OK) return bail(st);
+        if ((st = dalloc(h, (void**)&h->kd[a], (size_t)n * sizeof(cx<double>))) != SES_OK) return bail(st);
+        const unsigned gb = (unsigned)((n + 255) / 256);
+        if (prec == SES_C128)
+            build_twiddles<double><<<gb, 256, 0, h->stream>>>(n, reinterpret_cast<cx<double>*>(h->tw[a]));
+        else
+            build_twiddles<float><<<gb, 256, 0, h->stream>>>(n, reinterpret_cast<cx<float>*>(h->tw[a]));
+        build_axis_tables<<<gb, 256, 0, h->stream>>>(h->box[2 * a], h->box[2 * a + 1], n,
+                                                     with_tables ? dt : 0.0,
+                                                     with_tables ? mass : 1.0, h->kv[a], h->kd[a]);
+    }
+    if (cudaGetLastError() != cudaSuccess) return bail(fail(SES_EDEVICE, "axis table build failed"));
+    if (with_tables) {
+        if ((st = dalloc(h, (void**)&h->V, N * sizeof(double))) != SES_OK) return bail(st);
+        if ((st = dalloc(h, &h->vtab, N * h->esize)) != SES_OK) return bail(st);
+        if (cudaMemcpyAsync(h->V, V, N * sizeof(double), cudaMemcpyHostToDevice, h->stream) !=
+            cudaSuccess)
+            return bail(fail(SES_EDEVICE, "potential upload failed"));
+        st = prec == SES_C128 ? build_tables<double>(h) : build_tables<float>(h);
+        if (st != SES_OK) return bail(st);
+    }
+    if (psi0) {
+        if ((st = ses_gpu_write_psi(h, psi0)) != SES_OK) return bail(st);
+    } else {
+        if (cudaMemsetAsync(h->psi, 0, N * h->esize, h->stream) != cudaSuccess)
+            return bail(fail(SES_EDEVICE, "memset failed"));
+    }
+    if ((st = wait_bounded(h, 0)) != SES_OK) return bail(st);
+    *out = h;
+    return SES_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ses_version(void) { return "ses-b200 0.1 (sm_100a)"; }
+
+const char* ses_last_error(void) { return g_err.c_str(); }
+
+ses_status ses_device_count(int* out) {
+    if (!out) return fail(SES_EINVAL, "null output");
+    int c = 0;
+    const cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = 0;
+        return fail(SES_EDEVICE, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return SES_OK;
+}
+
+ses_status ses_gpu_create(const ses_grid_desc* grid, ses_precision prec, double dt, double mass,
+                          const double* V, const double* psi0, ses_handle* out) {
+    return create_impl(grid, prec, dt, mass, V, psi0, true, out);
+}
+
+ses_status ses_gpu_destroy(ses_handle h) {
+    SES_TRY(check_handle(h));
+    release(h);
+    return SES_OK;
+}
+
+ses_status ses_gpu_set_potential(ses_handle h, const double* V) {
+    SES_TRY(check_handle(h));
+    if (!V) return fail(SES_EINVAL, "potential pointer is null");
+    if (!h->with_tables) return fail(SES_EINVAL, "handle has no phase tables");
+    SES_CU(cudaMemcpyAsync(h->V, V, h->N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    SES_TRY(h->prec == SES_C128 ? build_tables<double>(h) : build_tables<float>(h));
+    return wait_bounded(h, 0);
+}
+
+ses_status ses_gpu_set_absorber_separable(ses_handle h, const double* mx, const double* my,
+                                          const double* mz) {
+    SES_TRY(check_handle(h));
+    const double* m[3] = {mx, my, mz};
+    if (!mx || !my || !mz) return fail(SES_EINVAL, "null mask profile");
+    SES_TRY(wait_bounded(h, 0));
+    drop_graphs(h);
+    if (h->maskfull) {
+        cudaFree(h->maskfull);
+        h->maskfull = nullptr;
+    }
+    for (int a = 0; a < 3; ++a) {
+        if (!h->mask1[a]) SES_TRY(dalloc(h, (void**)&h->mask1[a], (size_t)h->n[a] * sizeof(double)));
+        SES_CU(cudaMemcpy(h->mask1[a], m[a], (size_t)h->n[a] * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    h->has_mask = true;
+    return SES_OK;
+}
+
+ses_status ses_gpu_set_absorber(ses_handle h, const double* mask) {
+    SES_TRY(check_handle(h));
+    SES_TRY(wait_bounded(h, 0));
+    drop_graphs(h);
+    if (!mask) {
+        h->has_mask = false;
+        return SES_OK;
+    }
+    // Detect an exact per-axis product mask[i,j,k] == (mx[i]*my[j])*mz[k]:
+    // profiles read off the axis lines through the cell of largest mask value.
+    const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
+    long long best = 0;
+    for (long long f = 1; f < h->N; ++f)
+        if (mask[f] > mask[best]) best = f;
+    const int bi = (int)(best % nx), bj = (int)((best / nx) % ny), bk = (int)(best / ((long long)nx * ny));
+    bool separable = mask[best] == 1.0;
+    std::vector<double> mx(nx), my(ny), mz(nz);
+    if (separable) {
+        for (int i = 0; i < nx; ++i) mx[i] = mask[i + (long long)nx * (bj + (long long)ny * bk)];
+        for (int j = 0; j < ny; ++j) my[j] = mask[bi + (long long)nx * (j + (long long)ny * bk)];
+        for (int k = 0; k < nz; ++k) mz[k] = mask[bi + (long long)nx * (bj + (long long)ny * k)];
+        for (int k = 0; k < nz && separable; ++k)
+            for (int j = 0; j < ny && separable; ++j)
+                for (int i = 0; i < nx; ++i)
+                    if (mx[i] * my[j] * mz[k] != mask[i + (long long)nx * (j + (long long)ny * k)]) {
+                        separable = false;
+                        break;
+                    }
+    }
+    if (separable) return ses_gpu_set_absorber_separable(h, mx.data(), my.data(), mz.data());
+    for (int a = 0; a < 3; ++a) {
+        if (h->mask1[a]) cudaFree(h->mask1[a]);
+        h->mask1[a] = nullptr;
+    }
+    if (!h->maskfull) SES_TRY(dalloc(h, (void**)&h->maskfull, h->N * sizeof(double)));
+    SES_CU(cudaMemcpy(h->maskfull, mask, h->N * sizeof(double), cudaMemcpyHostToDevice));
+    h->has_mask = true;
+    return SES_OK;
+}
+
+ses_status ses_gpu_step(ses_handle h, int nsteps, int absorb) {
+    SES_TRY(check_handle(h));
+    if (!h->with_tables) return fail(SES_EINVAL, "handle has no phase tables");
+    if (nsteps < 0) return fail(SES_EINVAL, "nsteps must be >= 0");
+    if (nsteps == 0) return SES_OK;
+    const bool mask = absorb != 0 && h->has_mask;
+    return h->prec == SES_C128 ? enqueue_steps<double>(h, nsteps, mask)
+                               : enqueue_steps<float>(h, nsteps, mask);
+}
+
+ses_status ses_gpu_fft3(ses_handle h, int direction) {
+    SES_TRY(check_handle(h));
+    if (direction != 0 && direction != 1) return fail(SES_EINVAL, "direction must be 0 or 1");
+    return h->prec == SES_C128 ? enqueue_fft3<double>(h, h->psi, direction)
+                               : enqueue_fft3<float>(h, h->psi, direction);
+}
+
+ses_status ses_gpu_tables(ses_handle h, double* half_v, double* kin) {
+    SES_TRY(check_handle(h));
+    if (!h->with_tables) return fail(SES_EINVAL, "handle has no phase tables");
+    if (!half_v && !kin) return SES_OK;
+    void *dh = nullptr, *dk = nullptr;
+    ses_status st = SES_OK;
+    const size_t bytes = h->N * sizeof(cx<double>);
+    if (half_v && (st = dalloc(h, &dh, bytes)) != SES_OK) return st;
+    if (kin && (st = dalloc(h, &dk, bytes)) != SES_OK) {
+        cudaFree(dh);
+        return st;
+    }
+    const unsigned gb = (unsigned)std::min<long long>((h->N + 255) / 256, 148 * 32);
+    build_full_tables<<<gb, 256, 0, h->stream>>>(h->V, h->kv[0], h->kv[1], h->kv[2], h->n[0], h->n[1],
+                                                 h->N, h->dt, h->mass, (cx<double>*)dh, (cx<double>*)dk);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && dh) e = cudaMemcpyAsync(half_v, dh, bytes, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && dk) e = cudaMemcpyAsync(kin, dk, bytes, cudaMemcpyDeviceToHost, h->stream);
+    st = e == cudaSuccess ? wait_bounded(h, 0) : fail(SES_EDEVICE, cudaGetErrorString(e));
+    if (dh) {
+        cudaFree(dh);
+        h->bytes -= bytes;
+    }
+    if (dk) {
+        cudaFree(dk);
+        h->bytes -= bytes;
+    }
+    return st;
+}
+
+ses_status ses_gpu_dt(ses_handle h, double* dt) {
+    SES_TRY(check_handle(h));
+    if (!dt) return fail(SES_EINVAL, "null output");
+    *dt = h->dt;
+    return SES_OK;
+}
+
+ses_status ses_gpu_observe(ses_handle h, double xlo, double xhi, ses_observables* out) {
+    SES_TRY(check_handle(h));
+    if (!out) return fail(SES_EINVAL, "null output");
+    if (!h->with_tables) return fail(SES_EINVAL, "handle has no potential");
+    SES_TRY(h->prec == SES_C128 ? enqueue_observe<double>(h, xlo, xhi)
+                                : enqueue_observe<float>(h, xlo, xhi));
+    SES_TRY(wait_bounded(h, 0));
+    const double* r = h->hsums;
+    const double* k = h->hsums + kRedR;
+    const double dv = ((h->box[1] - h->box[0]) / h->n[0]) * ((h->box[3] - h->box[2]) / h->n[1]) *
+                      ((h->box[5] - h->box[4]) / h->n[2]);
+    auto ratio = [](double num, double den) { return den > 0.0 ? num / den : 0.0; };
+    out->norm = r[0] * dv;
+    out->energy_v = ratio(r[1], r[0]);
+    out->energy_t = ratio(k[1], k[0]);
+    out->energy = out->energy_v + out->energy_t;
+    out->p_range = r[2] * dv;
+    for (int a = 0; a < 3; ++a) {
+        out->mean_pos[a] = ratio(r[3 + a], r[0]);
+        const double var = ratio(r[6 + a], r[0]) - out->mean_pos[a] * out->mean_pos[a];
+        out->sigma_pos[a] = std::sqrt(std::max(0.0, var));
+        out->mean_mom[a] = ratio(k[2 + a], k[0]);
+    }
+    return SES_OK;
+}
+
+ses_status ses_gpu_write_psi(ses_handle h, const double* psi_in) {
+    SES_TRY(check_handle(h));
+    if (!psi_in) return fail(SES_EINVAL, "null psi");
+    const size_t N = (size_t)h->N;
+    if (h->prec == SES_C128) {
+        SES_CU(cudaMemcpyAsync(h->psi, psi_in, N * 16, cudaMemcpyHostToDevice, h->stream));
+        return wait_bounded(h, 0);
+    }
+    // C64: stage complex128 halves through the scratch field, round on device
+    const size_t half = (N + 1) / 2;
+    for (size_t off = 0; off < N; off += half) {
+        const size_t cnt = std::min(half, N - off);
+        SES_CU(cudaMemcpyAsync(h->scratch, psi_in + 2 * off, cnt * 16, cudaMemcpyHostToDevice, h->stream));
+        const unsigned gb = (unsigned)std::min<size_t>((cnt + 255) / 256, 148 * 32);
+        convert_kernel<double, float><<<gb, 256, 0, h->stream>>>(
+            reinterpret_cast<const cx<double>*>(h->scratch), reinterpret_cast<cx<float>*>(h->psi) + off,
+            (long long)cnt);
+        SES_CU(cudaGetLastError());
+    }
+    return wait_bounded(h, 0);
+}
+
+ses_status ses_gpu_read_psi(ses_handle h, double* psi_out) {
+    SES_TRY(check_handle(h));
+    if (!psi_out) return fail(SES_EINVAL, "null psi");
+    const size_t N = (size_t)h->N;
+    if (h->prec == SES_C128) {
+        SES_CU(cudaMemcpyAsync(psi_out, h->psi, N * 16, cudaMemcpyDeviceToHost, h->stream));
+        return wait_bounded(h, 0);
+    }
+    const size_t half = (N + 1) / 2;
+    for (size_t off = 0; off < N; off += half) {
+        const size_t cnt = std::min(half, N - off);
+        const unsigned gb = (unsigned)std::min<size_t>((cnt + 255) / 256, 148 * 32);
+        convert_kernel<float, double><<<gb, 256, 0, h->stream>>>(
+            reinterpret_cast<const cx<float>*>(h->psi) + off, reinterpret_cast<cx<double>*>(h->scratch),
+            (long long)cnt);
+        SES_CU(cudaGetLastError());
+        SES_CU(cudaMemcpyAsync(psi_out + 2 * off, h->scratch, cnt * 16, cudaMemcpyDeviceToHost, h->stream));
+    }
+    return wait_bounded(h, 0);
+}
+
+ses_status ses_gpu_sync(ses_handle h, int timeout_ms) {
+    SES_TRY(check_handle(h));
+    return wait_bounded(h, timeout_ms);
+}
+
+ses_status ses_gpu_set_stream(ses_handle h, void* cuda_stream) {
+    SES_TRY(check_handle(h));
+    SES_TRY(wait_bounded(h, 0));
+    h->stream = cuda_stream ? reinterpret_cast<cudaStream_t>(cuda_stream) : h->own;
+    return SES_OK;
+}
+
+ses_status ses_gpu_psi_device(ses_handle h, void** dptr, size_t* bytes) {
+    SES_TRY(check_handle(h));
+    if (dptr) *dptr = h->psi;
+    if (bytes) *bytes = (size_t)h->N * h->esize;
+    return SES_OK;
+}
+
+ses_status ses_gpu_footprint(ses_handle h, size_t* bytes) {
+    SES_TRY(check_handle(h));
+    if (!bytes) return fail(SES_EINVAL, "null output");
+    *bytes = h->bytes;
+    return SES_OK;
+}
+
+ses_status ses_fft3_host(const int32_t* n, ses_precision prec, double* data, int inverse) {
+    if (!n || !data) return fail(SES_EINVAL, "null argument");
+    ses_grid_desc g{};
+    g.x = ses_axis{0.0, 1.0, n[0]};
+    g.y = ses_axis{0.0, 1.0, n[1]};
+    g.z = ses_axis{0.0, 1.0, n[2]};
+    ses_handle h = nullptr;
+    SES_TRY(create_impl(&g, prec, 0.0, 1.0, nullptr, data, false, &h));
+    ses_status st = ses_gpu_fft3(h, inverse ? 1 : 0);
+    if (st == SES_OK) st = ses_gpu_read_psi(h, data);
+    release(h);
+    return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,506 @@
+// Axis-pass kernels of the Strang step and the device table builders.
+//
+// A Strang step of the reference, V/2 . F^-1 K F . V/2 (core/src/propagator.ixx:110-119),
+// is executed as a chain of axis passes over psi in HBM.  With the interior
+// half-kicks merged into full kicks (reference GPU batch, solver/src/vk_engine.ixx:611-633):
+//
+//   3D step:  X[inv x, V*M, fwd x]  Y[fwd y]  Z[fwd z, K/N, inv z]  Y[inv y]
+//   2D step:  X[inv x, V*M, fwd x]  Y[fwd y, K/N, inv y]
+//   1D step:  X[V*M, fwd x, K/N, inv x]
+//
+// so one step reads and writes psi 4 / 2 / 1 times and reads the potential
+// phase table once.  All diagonal factors (potential phase, absorbing mask,
+// kinetic phase, 1/N) are applied in FP64 whatever the storage precision.
+#pragma once
+
+#include "ses_fft.cuh"
+
+namespace sesk {
+
+constexpr int kEPTDev = 8;  // elements a thread holds per in-place Stockham stage
+
+enum DiagKind : int { DG_NONE = 0, DG_HALF = 1, DG_FULL = 2 };
+
+// Number of FP64 sums a k-space reduction produces:
+// [0] sum|phi|^2  [1] sum k^2/(2m)|phi|^2  [2..4] sum k_a |phi|^2
+constexpr int kRedK = 5;
+// Real-space sums: [0] sum|psi|^2 [1] sum V|psi|^2 [2] sum_{x in [a,b)}|psi|^2
+// [3..5] sum r_a|psi|^2 [6..8] sum r_a^2|psi|^2
+constexpr int kRedR = 9;
+
+struct Tables {
+    const void* vtab;          // C128: cis(-V dt/2) as cx<double>; C64: cis(-V dt/2) - 1 as cx<float>
+    const double* mask1[3];    // separable absorber profiles (all set or all null)
+    const double* maskfull;    // non-separable absorber (nullable)
+    const cx<double>* kd[3];   // per axis: cis(-k^2 dt/(2m)) - 1
+    const double* kv[3];       // per axis: wavenumbers (fftfreq layout)
+    double inv_mass;
+    double kscale;             // 1/N, folded into the kinetic multiply
+};
+
+template <typename T>
+struct PassArgs {
+    const cx<T>* src;
+    cx<T>* dst;
+    Geo g;
+    int axis;  // 0 = x (contiguous lines), 1 = y, 2 = z
+    int nx, ny, nz;
+    long long nlines;
+    // strided-axis addressing: line slot s -> base (s % nu) + (s / nu) * sw,
+    // element stride se.  For the x axis: base = s * nx, se = 1.
+    long long nu, sw, se;
+    FastDiv fnu, fny, fnx;
+    const cx<T>* tw;  // twiddles cis(-2 pi t / n), t < n
+    // run-time parts of the pass program (the structure is the kernel's MODE)
+    int d_load, d_mid, d_store;
+    int m_load, m_mid, m_store;
+    double out_scale;
+    Tables tb;
+    double* partials;
+};
+
+// psi * (potential phase) * (mask) at flat index f, coordinates (i, j, k).
+template <typename T>
+__device__ __forceinline__ cx<T> apply_diag(cx<T> v, int kind, int use_mask, long long f, int i, int j,
+                                            int k, const Tables& tb) {
+    cx<double> p = widen(v);
+    if (kind != DG_NONE) {
+        if constexpr (sizeof(T) == 8) {
+            const cx<double> h = reinterpret_cast<const cx<double>*>(tb.vtab)[f];
+            p = p * (kind == DG_FULL ? h * h : h);
+        } else {
+            cx<double> d = widen(reinterpret_cast<const cx<float>*>(tb.vtab)[f]);
+            if (kind == DG_FULL)  // (1 + d)^2 - 1 = 2d + d^2
+                d = mk<double>(2.0 * d.x + (d.x * d.x - d.y * d.y), 2.0 * d.y + 2.0 * d.x * d.y);
+            p = p + p * d;
+        }
+    }
+    if (use_mask) {
+        const double m = tb.maskfull ? tb.maskfull[f]
+                                     : tb.mask1[0][i] * tb.mask1[1][j] * tb.mask1[2][k];
+        p = mk<double>(p.x * m, p.y * m);
+    }
+    return narrow<T>(p);
+}
+
+// (1+a)(1+b) - 1 for the separable kinetic deltas
+__device__ __forceinline__ cx<double> dmul1(cx<double> a, cx<double> b) { return a + b + a * b; }
+
+// psi_k * K(k) / N followed by the conjugation that starts the inverse FFT.
+template <typename T>
+__device__ __forceinline__ cx<T> kinetic_conj(cx<T> v, cx<double> d, double kscale) {
+    cx<double> p = widen(v);
+    p = p + p * d;
+    return narrow<T>(mk<double>(p.x * kscale, -p.y * kscale));
+}
+
+template <int NR>
+__device__ __forceinline__ void block_reduce_store(double (&acc)[NR], double* out) {
+    __shared__ double red[32][NR];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+        double v = acc[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        acc[q] = v;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NR; ++q) red[warp][q] = acc[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < NR) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += red[w][threadIdx.x];
+        out[(size_t)blockIdx.x * NR + threadIdx.x] = s;
+    }
+}
+
+// Accumulate k-space sums of one element: axis wavenumber ka, other two
+// wavenumbers (kb, kc) in fixed axis slots.
+__device__ __forceinline__ void acc_k(double (&acc)[kRedK], double w, const double* k3,
+                                      double inv_mass) {
+    const double ksq = k3[0] * k3[0] + k3[1] * k3[1] + k3[2] * k3[2];
+    acc[0] += w;
+    acc[1] += 0.5 * ksq * inv_mass * w;
+    acc[2] += k3[0] * w;
+    acc[3] += k3[1] * w;
+    acc[4] += k3[2] * w;
+}
+
+// ---------------------------------------------------------------------------
+// Pass programs.  Each program is its own kernel so every kernel holds at most
+// two tile FFTs (register allocation stays local; no run-time program flags in
+// the butterfly loops).
+// ---------------------------------------------------------------------------
+enum XMode : int {
+    XM_FWD = 0,     // fwd x                                   (fft3 surface, energy copy)
+    XM_INV = 1,     // inv x, scaled                           (fft3 surface)
+    XM_START = 2,   // V/2, fwd x                              (first step of a batch)
+    XM_MID = 3,     // inv x, V (* M), fwd x                   (between steps)
+    XM_END = 4,     // inv x, V/2 (* M)                        (end of a batch)
+    XM_1D = 5,      // V/2 or V (* M), fwd x, K/N, inv x, [V/2 (* M)]   (x only axis)
+    XM_REDUCE = 6   // fwd x, k-space sums                     (1D energy)
+};
+enum SModeK : int { SM_FWD = 0, SM_INV = 1, SM_FUSED = 2, SM_REDUCE = 3 };
+
+// ---------------------------------------------------------------------------
+// Contiguous-axis (x) pass.  Tile = L consecutive x-lines, loaded and stored
+// with coalesced accesses; shared layout [l][e] with an odd pitch.
+// ---------------------------------------------------------------------------
+template <typename T, int MODE>
+__global__ void __launch_bounds__(512, 1) xpass_kernel(const PassArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ Geo g;  // stage tables are indexed at run time: keep them out of parameter space
+    if (threadIdx.x == 0) g = a.g;
+    cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+    const int n = a.g.n, L = a.g.L;
+    const long long m0 = (long long)blockIdx.x * L;
+    const int tile = L * n;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    constexpr bool kDiagLoad = MODE == XM_START || MODE == XM_1D;
+    constexpr bool kDiagStore = MODE == XM_END || MODE == XM_1D;
+
+    // load (coalesced), optional real-space diagonal
+    for (int idx = tid; idx < tile; idx += nt) {
+        const int l = (int)fdiv((uint32_t)idx, a.g.fn), e = idx - l * n;
+        const long long m = m0 + l;
+        cx<T> v = mk<T>((T)0, (T)0);
+        if (m < a.nlines) {
+            const long long f = m * n + e;
+            v = a.src[f];
+            if constexpr (kDiagLoad) {
+                if (a.d_load != DG_NONE || a.m_load) {
+                    const int k = (int)fdiv((uint32_t)m, a.fny);
+                    const int j = (int)(m - (long long)k * a.ny);
+                    v = apply_diag(v, a.d_load, a.m_load, f, e, j, k, a.tb);
+                }
+            }
+        }
+        sm[l * a.g.ls + e] = v;
+    }
+    __syncthreads();
+
+    auto lds = [&](int l, int e) -> cx<T> { return sm[l * g.ls + e]; };
+    auto sts = [&](int l, int e, cx<T> v) { sm[l * g.ls + e] = v; };
+
+    if constexpr (MODE == XM_INV || MODE == XM_MID || MODE == XM_END) {
+        const T s = (T)a.out_scale;
+        auto ldc = [&](int l, int e) -> cx<T> { return cconj(sm[l * g.ls + e]); };
+        auto stc = [&](int l, int e, cx<T> v) {
+            sm[l * g.ls + e] = MODE == XM_INV ? scale(cconj(v), s) : cconj(v);
+        };
+        fft_tile<T, kEPTDev, false, false>(g, sm, a.tw, ldc, stc);
+    }
+    if constexpr (MODE == XM_MID) {
+        if (a.d_mid != DG_NONE || a.m_mid) {
+            for (int idx = tid; idx < tile; idx += nt) {
+                const int l = (int)fdiv((uint32_t)idx, g.fn), e = idx - l * n;
+                const long long m = m0 + l;
+                if (m < a.nlines) {
+                    const int k = (int)fdiv((uint32_t)m, a.fny);
+                    const int j = (int)(m - (long long)k * a.ny);
+                    sm[l * g.ls + e] =
+                        apply_diag(sm[l * g.ls + e], a.d_mid, a.m_mid, m * n + e, e, j, k, a.tb);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if constexpr (MODE == XM_FWD || MODE == XM_START || MODE == XM_MID) {
+        fft_tile<T, kEPTDev, false, false>(g, sm, a.tw, lds, sts);
+    }
+    if constexpr (MODE == XM_1D) {
+        // x is the only transformed axis: fwd, K/N, inverse, all in the tile
+        auto stk = [&](int l, int e, cx<T> v) {
+            const long long m0l = m0 + l;
+            const long long m = m0l < a.nlines ? m0l : 0;
+            const int k = (int)fdiv((uint32_t)m, a.fny);
+            const int j = (int)(m - (long long)k * a.ny);
+            const cx<double> d = dmul1(dmul1(a.tb.kd[1][j], a.tb.kd[2][k]), a.tb.kd[0][e]);
+            sm[l * g.ls + e] = kinetic_conj(v, d, a.tb.kscale);
+        };
+        fft_tile<T, kEPTDev, false, false>(g, sm, a.tw, lds, stk);
+        auto stc = [&](int l, int e, cx<T> v) { sm[l * g.ls + e] = cconj(v); };
+        fft_tile<T, kEPTDev, false, false>(g, sm, a.tw, lds, stc);
+    }
+    if constexpr (MODE == XM_REDUCE) {
+        double acc[kRedK] = {0, 0, 0, 0, 0};
+        auto str = [&](int l, int e, cx<T> v) {
+            const long long m = m0 + l;
+            if (m < a.nlines) {
+                const int k = (int)fdiv((uint32_t)m, a.fny);
+                const int j = (int)(m - (long long)k * a.ny);
+                const double k3[3] = {a.tb.kv[0][e], a.tb.kv[1][j], a.tb.kv[2][k]};
+                const cx<double> p = widen(v);
+                acc_k(acc, p.x * p.x + p.y * p.y, k3, a.tb.inv_mass);
+            }
+        };
+        fft_tile<T, kEPTDev, false, false>(g, sm, a.tw, lds, str);
+        block_reduce_store<kRedK>(acc, a.partials);
+        return;
+    }
+
+    // store (coalesced), optional real-space diagonal
+    if constexpr (MODE != XM_REDUCE) for (int idx = tid; idx < tile; idx += nt) {
+        const int l = (int)fdiv((uint32_t)idx, g.fn), e = idx - l * n;
+        const long long m = m0 + l;
+        if (m < a.nlines) {
+            const long long f = m * n + e;
+            cx<T> v = sm[l * g.ls + e];
+            if constexpr (kDiagStore) {
+                if (a.d_store != DG_NONE || a.m_store) {
+                    const int k = (int)fdiv((uint32_t)m, a.fny);
+                    const int j = (int)(m - (long long)k * a.ny);
+                    v = apply_diag(v, a.d_store, a.m_store, f, e, j, k, a.tb);
+                }
+            }
+            a.dst[f] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Strided-axis (y or z) pass.  Tile = L line slots whose first elements are
+// consecutive in memory, so every element load/store of a warp is a
+// contiguous run.  Stage 0 reads HBM directly and the last stage writes HBM
+// directly; intermediate stages use the shared tile ([e][l] layout).
+// ---------------------------------------------------------------------------
+template <typename T, int MODE>
+__global__ void __launch_bounds__(512, 1) spass_kernel(const PassArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ Geo g;  // stage tables are indexed at run time: keep them out of parameter space
+    if (threadIdx.x == 0) g = a.g;
+    const int n = a.g.n, L = a.g.L;
+    cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);
+    // per-line data after the tile, 16-byte aligned: kinetic delta of the two
+    // other axes, their wavenumbers, and the line's base offset in psi
+    cx<double>* dother =
+        reinterpret_cast<cx<double>*>(smraw + (((size_t)L * n * sizeof(cx<T>) + 15) & ~(size_t)15));
+    double* kq = reinterpret_cast<double*>(dother + L);
+    long long* lbase = reinterpret_cast<long long*>(kq + 2 * L);
+    const long long s0 = (long long)blockIdx.x * L;
+    constexpr bool kLineInfo = MODE == SM_FUSED || MODE == SM_REDUCE;
+    // the two other axes, in increasing order: y-pass -> (x, z), z-pass -> (x, y)
+    const bool ypass = a.axis == 1;
+    const cx<double>* kd1 = a.tb.kd[0];
+    const cx<double>* kd2 = ypass ? a.tb.kd[2] : a.tb.kd[1];
+    const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
+    const double* kv1 = a.tb.kv[0];
+    const double* kv2 = ypass ? a.tb.kv[2] : a.tb.kv[1];
+    const double* kva = ypass ? a.tb.kv[1] : a.tb.kv[2];
+
+    for (int l = threadIdx.x; l < L; l += blockDim.x) {
+        const long long s = s0 + l;
+        long long base = -1;
+        int c1 = 0, c2 = 0;
+        if (s < a.nlines) {
+            const long long w = (long long)fdiv((uint32_t)s, a.fnu);
+            const long long u = s - w * a.nu;
+            base = u + w * a.sw;
+            if (ypass) {  // lines (i, k)
+                c1 = (int)u;
+                c2 = (int)w;
+            } else {  // z: lines (i, j), u = i + nx j
+                c2 = (int)fdiv((uint32_t)u, a.fnx);
+                c1 = (int)(u - (long long)c2 * a.nx);
+            }
+        }
+        lbase[l] = base;
+        if constexpr (kLineInfo) {
+            dother[l] = dmul1(kd1[c1], kd2[c2]);
+            kq[2 * l] = kv1[c1];
+            kq[2 * l + 1] = kv2[c2];
+        }
+    }
+    __syncthreads();
+
+    const long long se = a.se;
+    auto ldg = [&](int l, int e) -> cx<T> {
+        const long long b = lbase[l];
+        return b >= 0 ? a.src[b + e * se] : mk<T>((T)0, (T)0);
+    };
+    auto stg = [&](int l, int e, cx<T> v) {
+        const long long b = lbase[l];
+        if (b >= 0) a.dst[b + e * se] = v;
+    };
+
+    if constexpr (MODE == SM_FWD) {
+        fft_tile<T, kEPTDev, true, true>(g, sm, a.tw, ldg, stg);
+    } else if constexpr (MODE == SM_INV) {
+        const T s = (T)a.out_scale;
+        auto ldc = [&](int l, int e) -> cx<T> { return cconj(ldg(l, e)); };
+        auto stc = [&](int l, int e, cx<T> v) { stg(l, e, scale(cconj(v), s)); };
+        fft_tile<T, kEPTDev, true, true>(g, sm, a.tw, ldc, stc);
+    } else if constexpr (MODE == SM_FUSED) {
+        auto stk = [&](int l, int e, cx<T> v) {
+            const cx<double> d = dmul1(dother[l], kda[e]);
+            sm[l * g.ls + e * g.es] = kinetic_conj(v, d, a.tb.kscale);
+        };
+        fft_tile<T, kEPTDev, true, false>(g, sm, a.tw, ldg, stk);
+        auto lds = [&](int l, int e) -> cx<T> { return sm[l * g.ls + e * g.es]; };
+        auto stc = [&](int l, int e, cx<T> v) { stg(l, e, cconj(v)); };
+        fft_tile<T, kEPTDev, false, true>(g, sm, a.tw, lds, stc);
+    } else {  // SM_REDUCE
+        double acc[kRedK] = {0, 0, 0, 0, 0};
+        auto str = [&](int l, int e, cx<T> v) {
+            if (lbase[l] >= 0) {
+                const double ka = kva[e], kb = kq[2 * l + 1];
+                const double k3[3] = {kq[2 * l], ypass ? ka : kb, ypass ? kb : ka};
+                const cx<double> p = widen(v);
+                acc_k(acc, p.x * p.x + p.y * p.y, k3, a.tb.inv_mass);
+            }
+        };
+        fft_tile<T, kEPTDev, true, true>(g, sm, a.tw, ldg, str);
+        block_reduce_store<kRedK>(acc, a.partials);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Real-space observables: grid-stride FP64 sums, one partial row per CTA,
+// fixed grid -> deterministic.
+// ---------------------------------------------------------------------------
+struct ObsArgs {
+    long long N;
+    int nx, ny;
+    FastDiv fnx, fny;
+    double x0, hx, y0, hy, z0, hz;
+    double xlo, xhi;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) obs_real_kernel(const cx<T>* __restrict__ psi,
+                                                       const double* __restrict__ V, ObsArgs o,
+                                                       double* partials) {
+    double acc[kRedR];
+#pragma unroll
+    for (int q = 0; q < kRedR; ++q) acc[q] = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < o.N; idx += stride) {
+        const long long line = idx / o.nx;  // 64-bit: N may exceed 2^31
+        const int i = (int)(idx - line * o.nx);
+        const long long k = line / o.ny;
+        const int j = (int)(line - k * o.ny);
+        const cx<double> p = widen(psi[idx]);
+        const double w = p.x * p.x + p.y * p.y;
+        const double x = o.x0 + i * o.hx, y = o.y0 + j * o.hy, z = o.z0 + (double)k * o.hz;
+        acc[0] += w;
+        acc[1] += V[idx] * w;
+        if (x >= o.xlo && x < o.xhi) acc[2] += w;
+        acc[3] += x * w;
+        acc[4] += y * w;
+        acc[5] += z * w;
+        acc[6] += x * x * w;
+        acc[7] += y * y * w;
+        acc[8] += z * z * w;
+    }
+    block_reduce_store<kRedR>(acc, partials);
+}
+
+// Fixed-order final sum of per-CTA partial rows: out[q] = sum_b partials[b][q].
+__global__ void finalize_kernel(const double* __restrict__ partials, int nblocks, int nr, double* out) {
+    const int q = threadIdx.x;
+    if (q < nr) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * nr + q];
+        out[q] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 table builders.  Phase arguments use round-to-nearest intrinsics in the
+// reference's evaluation order (no FMA contraction), so theta is bitwise the
+// reference's: -0.5*V*dt (propagator.ixx:81) and
+// -0.5*(kx^2+ky^2+kz^2)/mass*dt (propagator.ixx:95-96).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double theta_v(double V, double dt) {
+    return __dmul_rn(__dmul_rn(-0.5, V), dt);
+}
+
+__device__ __forceinline__ double theta_k(double ksq, double mass, double dt) {
+    return __dmul_rn(__ddiv_rn(__dmul_rn(-0.5, ksq), mass), dt);
+}
+
+// cis(theta) - 1 without cancellation: (-2 sin^2(theta/2), sin(theta))
+__device__ __forceinline__ cx<double> cis_minus_one(double th) {
+    double s2, c2;
+    sincos(0.5 * th, &s2, &c2);
+    return mk<double>(-2.0 * s2 * s2, 2.0 * s2 * c2);
+}
+
+__global__ void build_vtab_c128(const double* __restrict__ V, cx<double>* out, long long N, double dt) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s, c;
+        sincos(theta_v(V[i], dt), &s, &c);
+        out[i] = mk<double>(c, s);
+    }
+}
+
+__global__ void build_vtab_c64(const double* __restrict__ V, cx<float>* out, long long N, double dt) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        out[i] = narrow<float>(cis_minus_one(theta_v(V[i], dt)));
+    }
+}
+
+// per-axis wavenumbers k_j = (2 pi / L) * (j if 2j < n else j - n)  (spectral.ixx:14-23)
+// and kinetic deltas cis(-k^2 dt/(2m)) - 1
+__global__ void build_axis_tables(double xmin, double xmax, int n, double dt, double mass,
+                                  double* kv, cx<double>* kd) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) {
+        const double dk = __ddiv_rn(2.0 * 3.14159265358979323846, __dsub_rn(xmax, xmin));
+        const int shifted = (2 * j < n) ? j : j - n;
+        const double k = __dmul_rn(dk, (double)shifted);
+        kv[j] = k;
+        kd[j] = cis_minus_one(theta_k(__dmul_rn(k, k), mass, dt));
+    }
+}
+
+template <typename T>
+__global__ void build_twiddles(int n, cx<T>* tw) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        double s, c;
+        sincospi(-2.0 * (double)t / (double)n, &s, &c);
+        tw[t] = mk<T>((T)c, (T)s);
+    }
+}
+
+// Full-N reference tables (propagator-tables surface).
+__global__ void build_full_tables(const double* __restrict__ V, const double* __restrict__ kvx,
+                                  const double* __restrict__ kvy, const double* __restrict__ kvz,
+                                  int nx, int ny, long long N, double dt, double mass,
+                                  cx<double>* half_v, cx<double>* kin) {
+    for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < N;
+         f += (long long)gridDim.x * blockDim.x) {
+        double s, c;
+        if (half_v) {
+            sincos(theta_v(V[f], dt), &s, &c);
+            half_v[f] = mk<double>(c, s);
+        }
+        if (kin) {
+            const long long line = f / nx;
+            const int i = (int)(f - line * nx);
+            const long long k = line / ny;
+            const int j = (int)(line - k * ny);
+            const double a = kvx[i], b = kvy[j], cz = kvz[k];
+            const double ksq = __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(cz, cz));
+            sincos(theta_k(ksq, mass, dt), &s, &c);
+            kin[f] = mk<double>(c, s);
+        }
+    }
+}
+
+template <typename S, typename D>
+__global__ void convert_kernel(const cx<S>* __restrict__ src, cx<D>* dst, long long N) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        dst[i] = mk<D>((D)src[i].x, (D)src[i].y);
+    }
+}
+
+}  // namespace sesk

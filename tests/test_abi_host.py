@@ -1,0 +1,196 @@
+"""Host-side checks that need no GPU: the C-ABI library loads and exports every
+symbol include/ses_gpu.h declares, argument errors are reported without a
+device, and the device index arithmetic (fast division, tile plans, shared
+memory carve-up) stays in bounds for every grid the tests and bench use."""
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "ses_gpu.h"
+
+
+def header_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"SES_API\s+[\w\s\*]+?\b(ses_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = header_symbols()
+    assert "ses_gpu_create" in syms and "ses_gpu_step" in syms and "ses_fft3_host" in syms
+    assert len(syms) >= 20
+
+
+def test_library_exports_every_header_symbol():
+    from shoeridingerequationsolver_b200 import _abi
+    lib = C.CDLL(str(_abi.LIB_PATH))
+    for s in header_symbols():
+        assert hasattr(lib, s), s
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_abi.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert set(header_symbols()) <= exported
+    # nothing beyond the declared C ABI leaks out of the library
+    assert {s for s in exported if s.startswith("ses_")} == set(header_symbols())
+
+
+def test_abi_binding_covers_header():
+    from shoeridingerequationsolver_b200 import _abi
+    assert sorted(_abi.EXPORTS) == header_symbols()
+
+
+def test_invalid_arguments_without_device():
+    import shoeridingerequationsolver_b200 as s
+    g = s.Grid3D(s.Grid1D(-1, 1, 7), s.Grid1D(-1, 1, 8), s.Grid1D(-1, 1, 8))
+    with pytest.raises(ValueError, match="2\\^a 3\\^b 5\\^c"):
+        s.SplitOperator3D(g, np.zeros(448), 0.1)
+    g2 = s.Grid3D(s.Grid1D(-1, 1, 8), s.Grid1D(-1, 1, 8), s.Grid1D(-1, 1, 8))
+    with pytest.raises(ValueError):
+        s.SplitOperator3D(g2, np.zeros(10), 0.1)          # potential size mismatch
+    with pytest.raises(ValueError):
+        s.SplitOperator3D(g2, np.zeros(512), 0.1, precision="fp16")
+    from shoeridingerequationsolver_b200 import _abi
+    h = C.c_void_p()
+    bad = _abi.GridDesc(_abi.Axis(1.0, 1.0, 8), _abi.Axis(0, 1, 8), _abi.Axis(0, 1, 8))
+    v = np.zeros(512)
+    st = _abi.lib.ses_gpu_create(C.byref(bad), 0, 0.1, 1.0, v.ctypes.data_as(C.POINTER(C.c_double)),
+                                 None, C.byref(h))
+    assert st == _abi.SES_EINVAL and "xmax > xmin" in _abi.last_error()
+    assert _abi.lib.ses_gpu_step(None, 1, 0) == _abi.SES_EINVAL
+
+
+def test_wavenumbers_and_grid_mirror(oracle):
+    import shoeridingerequationsolver_b200 as s
+    for (lo, hi, n) in [(0, 8, 8), (-1, 1, 1), (-13, -5, 8), (-40, 40, 256), (-10, 10, 48)]:
+        assert np.array_equal(s.wavenumbers(s.Grid1D(lo, hi, n)), oracle.wavenumbers(lo, hi, n))
+    g = s.Grid3D(s.Grid1D(0, 8, 16), s.Grid1D(0, 4, 8), s.Grid1D(-1, 1, 4))
+    assert g.size() == 512 and g.flat(3, 2, 1) == 3 + 16 * (2 + 8 * 1)
+    assert g.cell_volume() == 0.125
+
+
+# ---------------------------------------------------------------------------
+# Device index arithmetic, modelled on the CPU.  These restate the host plan
+# (ses_gpu.cu plan_pass / factor_radices) and the kernels' index ranges.
+
+def fastdiv(d):
+    if d <= 1:
+        return (d, 0, 0)
+    l = 0
+    while (1 << l) < d:
+        l += 1
+    p = 31 + l
+    return (d, ((1 << p) + d - 1) // d, p - 32)
+
+
+def fdiv(x, f):
+    d, m, s = f
+    return x if d <= 1 else ((x * m) >> 32) >> s
+
+
+def test_fastdiv_exact_below_2_31():
+    rng = np.random.default_rng(0)
+    divisors = list(range(1, 4200)) + [n * n for n in (48, 96, 160, 256, 512, 1024)]
+    for d in divisors:
+        f = fastdiv(d)
+        assert f[1] < 2 ** 32
+        xs = list(range(0, 600)) + [int(v) for v in rng.integers(0, 2 ** 31, 200)] + [2 ** 31 - 1]
+        for x in xs:
+            assert fdiv(x, f) == x // d, (d, x)
+
+
+EPT, MAXLOG = 8, 3
+
+
+def radices(n):
+    a = b = c = 0
+    m = n
+    while m % 2 == 0:
+        m //= 2
+        a += 1
+    while m % 3 == 0:
+        m //= 3
+        b += 1
+    while m % 5 == 0:
+        m //= 5
+        c += 1
+    if m != 1:
+        return None
+    r = []
+    if a:
+        p = (a + MAXLOG - 1) // MAXLOG
+        base, ex = a // p, a % p
+        r += [1 << (base + (1 if i < ex else 0)) for i in range(p)]
+    return r + [3] * b + [5] * c
+
+
+def plan(n, es, strided, nlines):
+    rad = radices(n)
+    L = 256 // es if strided else 128 // es
+    while L * n < 2048 and L < 256:
+        L *= 2
+    pitch = n if strided else (n + 1 if n % 2 == 0 else n)
+    while L > 1 and L * pitch * es > 64 * 1024:
+        L //= 2
+    while L > 1 and L // 2 >= nlines:
+        L //= 2
+
+    def threads(L):
+        t = 32
+        for R in rad:
+            t = max(t, -(-(L * n // R) // (EPT // R)))
+        return -(-t // 32) * 32
+    T = threads(L)
+    while T > 512 and L > 1:
+        L //= 2
+        T = threads(L)
+    smem = L * pitch * es
+    if strided:
+        smem = ((smem + 15) & ~15) + L * 40
+    return L, T, pitch, smem, rad
+
+
+GRIDS = [(8, 8, 8), (16, 8, 4), (8, 16, 4), (4, 4, 4), (64, 64, 64), (256, 256, 256),
+         (512, 512, 512), (48, 48, 48), (96, 96, 96), (160, 160, 160), (32, 32, 32),
+         (128, 128, 128), (512, 512, 1), (1024, 1024, 1), (4096, 1, 1), (1, 4, 1), (3, 5, 15),
+         (2, 2, 2), (48, 24, 20), (96, 20, 6), (512, 4, 2), (1024, 1, 1)]
+
+
+@pytest.mark.parametrize("dims", GRIDS)
+@pytest.mark.parametrize("es", [8, 16])
+def test_plans_stay_in_bounds(dims, es):
+    nx, ny, nz = dims
+    nlines = [ny * nz, nx * nz, nx * ny]
+    N = nx * ny * nz
+    for ax in range(3):
+        n = dims[ax]
+        L, T, pitch, smem, rad = plan(n, es, ax != 0, nlines[ax])
+        assert T <= 512 and L >= 1 and (L & (L - 1)) == 0
+        assert smem <= 200 * 1024
+        for R in rad:                     # butterflies per thread within the register budget
+            assert -(-(L * (n // R)) // T) <= EPT // R
+        if ax == 0:
+            assert (L - 1) * pitch + n - 1 < L * pitch
+        else:
+            assert (L - 1) + (n - 1) * L < L * n
+            assert ((L * n * es + 15) & ~15) % 16 == 0
+        # Stockham stage indices stay inside [0, n)
+        Ns = 1
+        for R in rad:
+            for j in range(n // R):
+                k = j % Ns
+                assert (R - 1) * k * (n // (Ns * R)) < n            # twiddle index
+                assert (j - k) * R + k + (R - 1) * Ns < n           # write index
+                assert j + (R - 1) * (n // R) < n                   # read index
+            Ns *= R
+        # last line's last element addresses inside psi
+        if ax == 0:
+            assert (nlines[0] - 1) * nx + nx - 1 < N
+        elif ax == 1:
+            assert (nx - 1) + (nz - 1) * nx * ny + (ny - 1) * nx < N
+        else:
+            assert (nx * ny - 1) + (nz - 1) * nx * ny < N
