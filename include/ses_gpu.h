@@ -146,6 +146,15 @@ SES_API ses_status ses_gpu_set_stream(ses_handle h, void* cuda_stream);
 /* Device pointer and byte size of the resident psi (complex128 or complex64,
  * x-fastest), for callers that keep data on the device. */
 SES_API ses_status ses_gpu_psi_device(ses_handle h, void** dptr, size_t* bytes);
+/* Engine::profile_step (vk_engine.ixx:700-774): run an nsteps Strang batch
+ * (absorb as in ses_gpu_step) launching every axis pass directly, with a CUDA
+ * event pair around each launch on the handle's stream.  pass_ms[8] receives
+ * the mean milliseconds per launch of:
+ *   [0] x pass between steps   [1] y forward   [2] last-axis fused (fwd, K/N, inv)
+ *   [3] y inverse              [4] x pass at batch start   [5] x pass at batch end
+ *   [6] total batch (first to last event)   [7] number of launches
+ * Unused kinds report 0.  psi advances exactly as with ses_gpu_step.  Blocks. */
+SES_API ses_status ses_gpu_profile_step(ses_handle h, int nsteps, int absorb, double* pass_ms);
 /* Device bytes held by the handle. */
 SES_API ses_status ses_gpu_footprint(ses_handle h, size_t* bytes);
 

@@ -92,8 +92,8 @@ class Field3D:
         self.grid = grid
         if data is None:
             self.data = np.zeros(grid.size(), dtype=np.complex128)
-        else:
-            self.data = np.ascontiguousarray(np.asarray(data, dtype=np.complex128).reshape(-1))
+        else:  # owns its values, like the reference's std::vector (field.ixx:52-66)
+            self.data = np.array(data, dtype=np.complex128, copy=True).reshape(-1)
             if self.data.size != grid.size():
                 raise ValueError("field size does not match the grid")
 
@@ -108,7 +108,7 @@ class Field1D:
     def __init__(self, grid: Grid1D, data=None):
         self.grid = grid
         self.data = (np.zeros(grid.n, dtype=np.complex128) if data is None else
-                     np.ascontiguousarray(np.asarray(data, dtype=np.complex128).reshape(-1)))
+                     np.array(data, dtype=np.complex128, copy=True).reshape(-1))
         if self.data.size != grid.n:
             raise ValueError("field size does not match the grid")
 
@@ -289,6 +289,17 @@ class SplitOperator3D:
         p, b = C.c_void_p(), C.c_size_t()
         check(lib.ses_gpu_psi_device(self._h, C.byref(p), C.byref(b)))
         return p.value, b.value
+
+    PASS_NAMES = ("x_mid", "y_fwd", "fused", "y_inv", "x_start", "x_end")
+
+    def profile_step(self, nsteps: int, absorb: bool = False) -> dict:
+        """Per-pass mean launch times (ms) of an nsteps batch (Engine::profile_step)."""
+        out = (C.c_double * 8)()
+        check(lib.ses_gpu_profile_step(self._h, int(nsteps), 1 if absorb else 0, out))
+        d = {k: out[i] for i, k in enumerate(self.PASS_NAMES)}
+        d["total_ms"] = out[6]
+        d["launches"] = int(out[7])
+        return d
 
     def footprint(self) -> int:
         b = C.c_size_t()

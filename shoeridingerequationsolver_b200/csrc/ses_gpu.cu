@@ -525,6 +525,102 @@ ses_status enqueue_observe(ses_solver* h, double xlo, double xhi) {
     return SES_OK;
 }
 
+// Per-pass timing of one batch (launch kinds: 0 x-mid, 1 y-fwd, 2 fused,
+// 3 y-inv, 4 x-start, 5 x-end), events on the handle's stream.
+template <typename T>
+ses_status profile_batch(ses_solver* h, int S, bool mask, double* out) {
+    cudaStream_t s = h->stream;
+    std::vector<std::pair<int, cudaEvent_t>> marks;  // kind of the launch that follows
+    auto mark = [&](int kind) -> ses_status {
+        cudaEvent_t e;
+        SES_CU(cudaEventCreate(&e));
+        SES_CU(cudaEventRecord(e, s));
+        marks.push_back({kind, e});
+        return SES_OK;
+    };
+    ses_status st = SES_OK;
+    auto run = [&]() -> ses_status {
+        if (h->last_axis == 0) {
+            for (int k = 0; k < S; ++k) {
+                XProg p;
+                p.mode = XM_1D;
+                p.d_load = k == 0 ? DG_HALF : DG_FULL;
+                p.m_load = k == 0 ? 0 : mask;
+                if (k == S - 1) {
+                    p.d_store = DG_HALF;
+                    p.m_store = mask;
+                }
+                SES_TRY(mark(k == 0 ? 4 : (k == S - 1 ? 5 : 0)));
+                SES_TRY(pass_x<T>(h, h->psi, h->psi, p, s));
+            }
+            return mark(-1);
+        }
+        auto mids = [&]() -> ses_status {
+            if (h->last_axis == 2) {
+                if (h->n[1] > 1) {
+                    SES_TRY(mark(1));
+                    SES_TRY(pass_s<T>(h, 1, h->psi, h->psi, SM_FWD, 1.0, s));
+                }
+                SES_TRY(mark(2));
+                SES_TRY(pass_s<T>(h, 2, h->psi, h->psi, SM_FUSED, 1.0, s));
+                if (h->n[1] > 1) {
+                    SES_TRY(mark(3));
+                    SES_TRY(pass_s<T>(h, 1, h->psi, h->psi, SM_INV, 1.0, s));
+                }
+            } else {
+                SES_TRY(mark(2));
+                SES_TRY(pass_s<T>(h, 1, h->psi, h->psi, SM_FUSED, 1.0, s));
+            }
+            return SES_OK;
+        };
+        XProg start;
+        start.mode = XM_START;
+        start.d_load = DG_HALF;
+        SES_TRY(mark(4));
+        SES_TRY(pass_x<T>(h, h->psi, h->psi, start, s));
+        SES_TRY(mids());
+        for (int k = 1; k < S; ++k) {
+            XProg p;
+            p.mode = XM_MID;
+            p.d_mid = DG_FULL;
+            p.m_mid = mask;
+            SES_TRY(mark(0));
+            SES_TRY(pass_x<T>(h, h->psi, h->psi, p, s));
+            SES_TRY(mids());
+        }
+        XProg end;
+        end.mode = XM_END;
+        end.d_store = DG_HALF;
+        end.m_store = mask;
+        SES_TRY(mark(5));
+        SES_TRY(pass_x<T>(h, h->psi, h->psi, end, s));
+        return mark(-1);
+    };
+    st = run();
+    if (st == SES_OK) st = wait_bounded(h, 60000);
+    double sum[6] = {0, 0, 0, 0, 0, 0};
+    int cnt[6] = {0, 0, 0, 0, 0, 0};
+    if (st == SES_OK) {
+        for (size_t i = 0; i + 1 < marks.size(); ++i) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, marks[i].second, marks[i + 1].second) != cudaSuccess) {
+                st = fail(SES_EDEVICE, "event timing failed");
+                break;
+            }
+            sum[marks[i].first] += ms;
+            cnt[marks[i].first] += 1;
+        }
+        float total = 0.f;
+        if (st == SES_OK && marks.size() >= 2)
+            cudaEventElapsedTime(&total, marks.front().second, marks.back().second);
+        for (int k = 0; k < 6; ++k) out[k] = cnt[k] ? sum[k] / cnt[k] : 0.0;
+        out[6] = total;
+        out[7] = (double)(marks.size() - 1);
+    }
+    for (auto& m : marks) cudaEventDestroy(m.second);
+    return st;
+}
+
 ses_status check_handle(ses_handle h) {
     if (!h) return fail(SES_EINVAL, "null handle");
     return SES_OK;
@@ -601,7 +697,9 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
 
     ses_status st;
     if ((st = dalloc(h, &h->psi, N * h->esize)) != SES_OK) return bail(st);
-    if ((st = dalloc(h, &h->scratch, N * h->esize)) != SES_OK) return bail(st);
+    // scratch: the k-space copy for observables, and the staging area for
+    // complex128 halves on C64 upload/readback ((N+1)/2 * 16 B <= N*8 + 16 B)
+    if ((st = dalloc(h, &h->scratch, N * h->esize + 16)) != SES_OK) return bail(st);
     h->partial_rows = rows;
     if ((st = dalloc(h, (void**)&h->partials, rows * kRedR * sizeof(double))) != SES_OK) return bail(st);
     if ((st = dalloc(h, (void**)&h->dsums, 32 * sizeof(double))) != SES_OK) return bail(st);
@@ -884,6 +982,17 @@ ses_status ses_gpu_psi_device(ses_handle h, void** dptr, size_t* bytes) {
     if (dptr) *dptr = h->psi;
     if (bytes) *bytes = (size_t)h->N * h->esize;
     return SES_OK;
+}
+
+ses_status ses_gpu_profile_step(ses_handle h, int nsteps, int absorb, double* pass_ms) {
+    SES_TRY(check_handle(h));
+    if (!pass_ms) return fail(SES_EINVAL, "null output");
+    if (!h->with_tables) return fail(SES_EINVAL, "handle has no phase tables");
+    if (nsteps < 1) return fail(SES_EINVAL, "nsteps must be >= 1");
+    for (int k = 0; k < 8; ++k) pass_ms[k] = 0.0;
+    const bool mask = absorb != 0 && h->has_mask;
+    return h->prec == SES_C128 ? profile_batch<double>(h, nsteps, mask, pass_ms)
+                               : profile_batch<float>(h, nsteps, mask, pass_ms);
 }
 
 ses_status ses_gpu_footprint(ses_handle h, size_t* bytes) {

@@ -1,0 +1,187 @@
+"""Host-side builders of potentials, absorbers and initial packets (FP64, numpy).
+
+Vectorised restatements of the reference builders (core/src/potential.ixx,
+core/src/wavepacket.ixx) plus the inputs of the benchmarked workloads.  They
+produce the arrays handed to SplitOperator3D; the propagation itself runs on
+the device.  Layout: flat x-fastest, index i + nx*(j + ny*k).
+
+Absorber profile (new; the reference has only a sin^2 ramp,
+potential.ixx:192-233): within `width` of a wall, at wall distance d,
+    m(d) = cos(pi/2 * (1 - d/width))^(1/8)   (evaluated as sin(pi d/(2 width))^(1/8),
+                                              which is exactly 0 on the wall)
+and 1 further in; 3D masks are products of the per-axis profiles.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .core import Grid1D, Grid3D
+
+K_COULOMB_CELL_AVERAGE = 2.3800774  # potential.ixx:99-100
+SEED_BASE = 0x5E5B200
+
+
+def _axes(g: Grid3D):
+    return (g.x.coords()[None, None, :], g.y.coords()[None, :, None], g.z.coords()[:, None, None])
+
+
+def harmonic(g: Grid3D, omega: float, c=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """0.5 w^2 |r - c|^2 (potential.ixx:35-49)."""
+    x, y, z = _axes(g)
+    dx, dy, dz = x - c[0], y - c[1], z - c[2]
+    return (0.5 * omega * omega * (dx * dx + dy * dy + dz * dz)).reshape(-1)
+
+
+def regularized_coulomb(g: Grid3D, Z: float, c=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Bare -Z/r, nucleus cell -Z * 2.3800774 / h (potential.ixx:134-151)."""
+    h = g.x.spacing()
+    x, y, z = _axes(g)
+    dx, dy, dz = x - c[0], y - c[1], z - c[2]
+    r = np.sqrt(dx * dx + dy * dy + dz * dz)
+    with np.errstate(divide="ignore"):
+        v = np.where(r < 1e-6 * h, -Z * K_COULOMB_CELL_AVERAGE / h, -Z / r)
+    return v.reshape(-1)
+
+
+def stark_fold(g: Grid3D, v: np.ndarray, e_field: float) -> np.ndarray:
+    """V += E z (hydrogen_director.ixx:1359-1370)."""
+    z = g.z.coords()[:, None, None]
+    return (v.reshape(g.shape) + e_field * z).reshape(-1)
+
+
+def barrier(g: Grid3D, v0: float, x_lo: float, x_hi: float) -> np.ndarray:
+    """v0 on the slab x in [x_lo, x_hi) (potential.ixx:114-129)."""
+    x = g.x.coords()
+    row = np.where((x >= x_lo) & (x < x_hi), v0, 0.0)
+    return np.broadcast_to(row[None, None, :], g.shape).reshape(-1).copy()
+
+
+def stadium(g: Grid3D, half_len: float, r: float, v_out: float) -> np.ndarray:
+    """v_out where the stadium SDF > 0 in the x-y plane (billiard2d_director.ixx:26-29)."""
+    x = g.x.coords()[None, None, :]
+    y = g.y.coords()[None, :, None]
+    cx = np.clip(x, -half_len, half_len)
+    sdf = np.hypot(x - cx, y) - r
+    v = np.where(sdf > 0.0, v_out, 0.0)
+    return np.broadcast_to(v, g.shape).reshape(-1).copy()
+
+
+def morse(g: Grid1D, d: float, alpha: float, x0: float) -> np.ndarray:
+    q = 1.0 - np.exp(-alpha * (g.coords() - x0))
+    return d * q * q
+
+
+def double_well(g: Grid1D, vb: float, a: float) -> np.ndarray:
+    s = g.coords() / a
+    q = s * s - 1.0
+    return vb * q * q
+
+
+def poschl_teller(g: Grid1D, v0: float, a: float, x0: float = 0.0) -> np.ndarray:
+    c = np.cosh((g.coords() - x0) / a)
+    return -v0 / (c * c)
+
+
+def mask_profile(g: Grid1D, width: float, profile: str = "cos8") -> np.ndarray:
+    """Per-axis absorber: 'sin2' is the reference ramp, 'cos8' the cos^(1/8) ramp."""
+    if g.n == 1:
+        return np.ones(1)
+    x = g.coords()
+    d = np.minimum(x - g.xmin, g.xmax - x)
+    s = np.sin(0.5 * 3.14159265358979323846 * np.minimum(d, width) / width)
+    m = s * s if profile == "sin2" else np.power(s, 0.125)
+    return np.where(d >= width, 1.0, m)
+
+
+def mask_profiles(g: Grid3D, frac: float, profile: str = "cos8"):
+    """Absorber on the outer `frac` of each axis: width = frac * axis length."""
+    return tuple(mask_profile(a, frac * (a.xmax - a.xmin), profile) for a in (g.x, g.y, g.z))
+
+
+def gaussian(g: Grid3D, r0, sigma, k0) -> np.ndarray:
+    """Separable Gaussian packet times e^{i k0.r}, normalised on the grid (wavepacket.ixx:29-49)."""
+    def env(u, u0, s):
+        return math.pow(2.0 * math.pi * s * s, -0.25) * np.exp(-(u - u0) * (u - u0) / (4.0 * s * s))
+    x, y, z = _axes(g)
+    amp = env(x, r0[0], sigma[0]) * env(y, r0[1], sigma[1]) * env(z, r0[2], sigma[2])
+    ph = k0[0] * x + k0[1] * y + k0[2] * z
+    psi = (amp * np.exp(1j * ph)).reshape(-1)
+    return normalized(g, psi)
+
+
+def normalized(g: Grid3D, psi: np.ndarray) -> np.ndarray:
+    n2 = float(np.vdot(psi, psi).real) * g.cell_volume()
+    return psi / math.sqrt(n2) if n2 > 0 else psi
+
+
+def gaussian_superposition(g: Grid3D, rng: np.random.Generator, m: int = 4, radius: float = 5.0,
+                           sigma_range=(0.8, 2.0)) -> tuple[np.ndarray, list]:
+    """Normalised sum of m isotropic Gaussians: centres uniform in |c| < radius
+    (rejection), widths U[sigma_range], phases U[0, 2 pi), zero momentum."""
+    psi = np.zeros(g.size(), dtype=np.complex128)
+    parts = []
+    for _ in range(m):
+        while True:
+            c = rng.uniform(-radius, radius, 3)
+            if np.dot(c, c) < radius * radius:
+                break
+        s = float(rng.uniform(*sigma_range))
+        phi = float(rng.uniform(0.0, 2.0 * math.pi))
+        psi += np.exp(1j * phi) * gaussian(g, c, (s, s, s), (0.0, 0.0, 0.0))
+        parts.append({"centre": c.tolist(), "sigma": s, "phase": phi})
+    return normalized(g, psi), parts
+
+
+def cube_grid(lo: float, hi: float, n: int) -> Grid3D:
+    a = Grid1D(lo, hi, n)
+    return Grid3D(a, a, a)
+
+
+@dataclass
+class Workload:
+    name: str
+    grid: Grid3D
+    V: np.ndarray
+    psi0: np.ndarray
+    dt: float
+    steps: int
+    mask: tuple | None = None
+    mass: float = 1.0
+    observe_every: int = 100
+    x_range: tuple = (-math.inf, math.inf)
+    meta: dict = field(default_factory=dict)
+
+
+def config_c1() -> Workload:
+    """Plain FP64 single instance: 64^3 harmonic trap on [-10,10)^3, packet at (2,0,0), dt 0.005."""
+    g = cube_grid(-10.0, 10.0, 64)
+    return Workload("c1_harmonic_64", g, harmonic(g, 1.0), gaussian(g, (2, 0, 0), (1, 1, 1), (0, 0, 0)),
+                    0.005, 2000, observe_every=100)
+
+
+def config_c2(n: int = 256) -> Workload:
+    """Regularized Coulomb Z=1 + Stark 0.01 z on [-40,40)^3, seeded 4-Gaussian superposition,
+    cos^(1/8) absorber on the outer 10% of each axis, dt 0.01, 1000 steps."""
+    g = cube_grid(-40.0, 40.0, n)
+    rng = np.random.default_rng(SEED_BASE + 1)
+    V = stark_fold(g, regularized_coulomb(g, 1.0), 0.01)
+    psi0, parts = gaussian_superposition(g, rng)
+    return Workload(f"c2_coulomb_stark_{n}", g, V, psi0, 0.01, 1000, mask=mask_profiles(g, 0.10),
+                    observe_every=100, meta={"seed": SEED_BASE + 1, "packets": parts})
+
+
+def config_c3(n: int = 512) -> Workload:
+    """3D tunnelling on [-60,60)^3: barrier of thickness 2 at x=0 with height U[1,5]
+    (seeded), packet sigma 3 at x=-20 with k0 = (3,0,0), cos^(1/8) absorber on the
+    outer 8%, dt 0.002, 500 steps, transmitted P(x >= 1) every 50 steps."""
+    g = cube_grid(-60.0, 60.0, n)
+    rng = np.random.default_rng(SEED_BASE + 2)
+    v0 = float(rng.uniform(1.0, 5.0))
+    return Workload(f"c3_tunnel_{n}", g, barrier(g, v0, -1.0, 1.0),
+                    gaussian(g, (-20.0, 0.0, 0.0), (3.0, 3.0, 3.0), (3.0, 0.0, 0.0)), 0.002, 500,
+                    mask=mask_profiles(g, 0.08), observe_every=50, x_range=(1.0, math.inf),
+                    meta={"seed": SEED_BASE + 2, "barrier_height": v0})
