@@ -1,0 +1,178 @@
+// ses_gpu.hpp -- C++ adapter over the C ABI (ses_gpu.h) with the reference
+// core's call surface, so director code written against ses::SplitOperator3D
+// (core/src/propagator.ixx), ses::fft/ifft (core/src/fft.ixx) and ses::Field3D
+// (core/src/field.ixx) switches to the B200 path by changing a namespace.
+//
+// Error behaviour follows the reference: unsupported sizes throw
+// std::invalid_argument (fft.ixx:42-44); out-of-memory throws std::bad_alloc;
+// device errors and expired bounded waits throw std::runtime_error.
+#pragma once
+
+#include <complex>
+#include <cstddef>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "ses_gpu.h"
+
+namespace ses::gpu {
+
+using cd = std::complex<double>;
+
+inline void check(ses_status s) {
+    if (s == SES_OK) return;
+    const std::string msg = ses_last_error();
+    if (s == SES_EINVAL) throw std::invalid_argument(msg);
+    if (s == SES_ENOMEM) throw std::bad_alloc();
+    throw std::runtime_error("ses_gpu: " + msg);
+}
+
+// Grid1D / Grid3D (core/src/grid.ixx:10-30)
+struct Grid1D {
+    double xmin{};
+    double xmax{};
+    int n{};
+    constexpr int size() const noexcept { return n; }
+    constexpr double spacing() const noexcept { return (xmax - xmin) / n; }
+    constexpr double coord(int i) const noexcept { return xmin + i * spacing(); }
+};
+
+struct Grid3D {
+    Grid1D x{}, y{}, z{};
+    constexpr int size() const noexcept { return x.n * y.n * z.n; }
+    constexpr int flat(int i, int j, int k) const noexcept { return i + x.n * (j + y.n * k); }
+    constexpr double cell_volume() const noexcept {
+        return x.spacing() * y.spacing() * z.spacing();
+    }
+    ses_grid_desc desc() const noexcept {
+        return ses_grid_desc{{x.xmin, x.xmax, x.n}, {y.xmin, y.xmax, y.n}, {z.xmin, z.xmax, z.n}};
+    }
+};
+
+// Field3D (core/src/field.ixx:47-66): owns complex128 values, x-fastest
+class Field3D {
+public:
+    explicit Field3D(Grid3D g) : grid_(g), data_(static_cast<std::size_t>(g.size())) {}
+    int size() const noexcept { return grid_.size(); }
+    const Grid3D& grid() const noexcept { return grid_; }
+    cd& operator()(int i, int j, int k) noexcept { return data_[grid_.flat(i, j, k)]; }
+    const cd& operator()(int i, int j, int k) const noexcept { return data_[grid_.flat(i, j, k)]; }
+    std::vector<cd>& data() noexcept { return data_; }
+    const std::vector<cd>& data() const noexcept { return data_; }
+
+private:
+    Grid3D grid_;
+    std::vector<cd> data_;
+};
+
+inline const double* raw(const std::vector<cd>& v) { return reinterpret_cast<const double*>(v.data()); }
+inline double* raw(std::vector<cd>& v) { return reinterpret_cast<double*>(v.data()); }
+
+// fft(Field3D&) / ifft(Field3D&) (fft.ixx:102-188) through the device
+inline void fft(Field3D& f, ses_precision p = SES_C128) {
+    const int32_t n[3] = {f.grid().x.n, f.grid().y.n, f.grid().z.n};
+    check(ses_fft3_host(n, p, raw(f.data()), 0));
+}
+inline void ifft(Field3D& f, ses_precision p = SES_C128) {
+    const int32_t n[3] = {f.grid().x.n, f.grid().y.n, f.grid().z.n};
+    check(ses_fft3_host(n, p, raw(f.data()), 1));
+}
+// fft(std::vector<cd>&) / ifft (fft.ixx:75-98)
+inline void fft(std::vector<cd>& a, ses_precision p = SES_C128) {
+    const int32_t n[3] = {static_cast<int32_t>(a.size()), 1, 1};
+    check(ses_fft3_host(n, p, raw(a), 0));
+}
+inline void ifft(std::vector<cd>& a, ses_precision p = SES_C128) {
+    const int32_t n[3] = {static_cast<int32_t>(a.size()), 1, 1};
+    check(ses_fft3_host(n, p, raw(a), 1));
+}
+
+// SplitOperator3D (propagator.ixx:68-134) plus the resident engine calls of
+// the reference GPU engine (vk_engine.ixx: upload_state, step(n, absorb),
+// set_absorber, readback, norm/energy).
+class SplitOperator3D {
+public:
+    SplitOperator3D(const Grid3D& g, const std::vector<double>& potential, double dt,
+                    double mass = 1.0, ses_precision prec = SES_C128)
+        : grid_(g), dt_(dt) {
+        if (static_cast<int>(potential.size()) != g.size())
+            throw std::invalid_argument("potential size does not match the grid");
+        const ses_grid_desc d = g.desc();
+        check(ses_gpu_create(&d, prec, dt, mass, potential.data(), nullptr, &h_));
+    }
+    SplitOperator3D(const SplitOperator3D&) = delete;
+    SplitOperator3D& operator=(const SplitOperator3D&) = delete;
+    SplitOperator3D(SplitOperator3D&& o) noexcept : grid_(o.grid_), dt_(o.dt_), h_(o.h_) { o.h_ = nullptr; }
+    ~SplitOperator3D() {
+        if (h_) ses_gpu_destroy(h_);
+    }
+
+    double dt() const noexcept { return dt_; }
+
+    std::vector<cd> half_potential_phase() const {
+        std::vector<cd> t(static_cast<std::size_t>(grid_.size()));
+        check(ses_gpu_tables(h_, raw(t), nullptr));
+        return t;
+    }
+    std::vector<cd> kinetic_phase() const {
+        std::vector<cd> t(static_cast<std::size_t>(grid_.size()));
+        check(ses_gpu_tables(h_, nullptr, raw(t)));
+        return t;
+    }
+
+    // In place on a caller-owned field, like the reference (propagator.ixx:110-119).
+    void step(Field3D& psi, int nsteps = 1) const {
+        if (psi.size() != grid_.size()) throw std::invalid_argument("field does not match the grid");
+        check(ses_gpu_write_psi(h_, raw(psi.data())));
+        check(ses_gpu_step(h_, nsteps, 0));
+        check(ses_gpu_read_psi(h_, raw(psi.data())));
+    }
+
+    // ---- resident engine surface ----
+    void upload_state(const std::vector<cd>& psi) { check(ses_gpu_write_psi(h_, raw(psi))); }
+    void advance(int nsteps, bool absorb = false) { check(ses_gpu_step(h_, nsteps, absorb ? 1 : 0)); }
+    std::vector<cd> readback() const {
+        std::vector<cd> out(static_cast<std::size_t>(grid_.size()));
+        check(ses_gpu_read_psi(h_, raw(out)));
+        return out;
+    }
+    void set_absorber(const std::vector<double>& mask) { check(ses_gpu_set_absorber(h_, mask.data())); }
+    void clear_absorber() { check(ses_gpu_set_absorber(h_, nullptr)); }
+    void set_potential(const std::vector<double>& v) { check(ses_gpu_set_potential(h_, v.data())); }
+    ses_observables observe(double xlo = -1e300, double xhi = 1e300) const {
+        ses_observables o{};
+        check(ses_gpu_observe(h_, xlo, xhi, &o));
+        return o;
+    }
+    void sync(int timeout_ms = 0) const { check(ses_gpu_sync(h_, timeout_ms)); }
+    ses_handle handle() const noexcept { return h_; }
+
+private:
+    Grid3D grid_;
+    double dt_;
+    ses_handle h_ = nullptr;
+};
+
+// SplitOperator1D (propagator.ixx:21-66): the 3D engine on n x 1 x 1
+class SplitOperator1D {
+public:
+    SplitOperator1D(const Grid1D& g, const std::vector<double>& potential, double dt,
+                    ses_precision prec = SES_C128)
+        : op_(Grid3D{g, Grid1D{0.0, 1.0, 1}, Grid1D{0.0, 1.0, 1}}, potential, dt, 1.0, prec), n_(g.n) {}
+    double dt() const noexcept { return op_.dt(); }
+    void step(std::vector<cd>& psi, int nsteps = 1) const {
+        if (static_cast<int>(psi.size()) != n_) throw std::invalid_argument("field does not match the grid");
+        check(ses_gpu_write_psi(op_.handle(), raw(psi)));
+        check(ses_gpu_step(op_.handle(), nsteps, 0));
+        check(ses_gpu_read_psi(op_.handle(), raw(psi)));
+    }
+
+private:
+    SplitOperator3D op_;
+    int n_;
+};
+
+}  // namespace ses::gpu

@@ -17,8 +17,9 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libses_b200.so"
-SOURCES = ["ses_gpu.cu"]
-HEADERS = ["ses_fft.cuh", "ses_pass.cuh"]
+SOURCES = ["ses_gpu.cu", "ses_plans_small.cu", "ses_plans_mixed.cu", "ses_plans_256.cu",
+           "ses_plans_large.cu"]
+HEADERS = ["ses_fft.cuh", "ses_pass.cuh", "ses_pass2.cuh", "ses_plans.cuh", "ses_aux.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-shared",
@@ -39,13 +40,25 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
+    """Compile each translation unit in parallel, then link the shared library."""
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), *ARCH, *FLAGS, "-I", str(ROOT / "include"), "-I", str(CSRC)]
-    if ptxas_verbose:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [str(CSRC / s) for s in SOURCES] + ["-o", str(LIB)]
-    subprocess.run(cmd, check=True)
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    compile_flags = [f for f in FLAGS if f != "-shared"]
+    procs = []
+    for src in SOURCES:
+        obj = objdir / (Path(src).stem + ".o")
+        cmd = [nvcc(), *ARCH, *compile_flags, "-I", str(ROOT / "include"), "-I", str(CSRC), "-c",
+               str(CSRC / src), "-o", str(obj)]
+        if ptxas_verbose:
+            cmd += ["-Xptxas", "-v"]
+        procs.append((obj, subprocess.Popen(cmd)))
+    failed = [str(o) for o, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError(f"nvcc failed for {failed}")
+    link = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *[str(o) for o, _ in procs], "-o", str(LIB)]
+    subprocess.run(link, check=True)
     return LIB
 
 

@@ -1,0 +1,106 @@
+// Non-template kernels of the solver (table builders, final reductions).
+// Included by ses_gpu.cu only: __global__ functions defined here have one
+// definition in the library.
+#pragma once
+
+#include "ses_pass.cuh"
+
+namespace sesk {
+
+// Fixed-order final sum of per-CTA partial rows: out[q] = sum_b partials[b][q].
+__global__ void finalize_kernel(const double* __restrict__ partials, int nblocks, int nr, double* out) {
+    const int q = threadIdx.x;
+    if (q < nr) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * nr + q];
+        out[q] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 table builders.  Phase arguments use round-to-nearest intrinsics in the
+// reference's evaluation order (no FMA contraction), so theta is bitwise the
+// reference's: -0.5*V*dt (propagator.ixx:81) and
+// -0.5*(kx^2+ky^2+kz^2)/mass*dt (propagator.ixx:95-96).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double theta_v(double V, double dt) {
+    return __dmul_rn(__dmul_rn(-0.5, V), dt);
+}
+
+__device__ __forceinline__ double theta_k(double ksq, double mass, double dt) {
+    return __dmul_rn(__ddiv_rn(__dmul_rn(-0.5, ksq), mass), dt);
+}
+
+// cis(theta) - 1 without cancellation: (-2 sin^2(theta/2), sin(theta))
+__device__ __forceinline__ cx<double> cis_minus_one(double th) {
+    double s2, c2;
+    sincos(0.5 * th, &s2, &c2);
+    return mk<double>(-2.0 * s2 * s2, 2.0 * s2 * c2);
+}
+
+__global__ void build_vtab_c128(const double* __restrict__ V, cx<double>* out, long long N, double dt) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s, c;
+        sincos(theta_v(V[i], dt), &s, &c);
+        out[i] = mk<double>(c, s);
+    }
+}
+
+__global__ void build_vtab_c64(const double* __restrict__ V, cx<float>* out, long long N, double dt) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        out[i] = narrow<float>(cis_minus_one(theta_v(V[i], dt)));
+    }
+}
+
+// per-axis wavenumbers k_j = (2 pi / L) * (j if 2j < n else j - n)  (spectral.ixx:14-23)
+// and kinetic deltas cis(-k^2 dt/(2m)) - 1
+__global__ void build_axis_tables(double xmin, double xmax, int n, double dt, double mass,
+                                  double* kv, cx<double>* kd) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) {
+        const double dk = __ddiv_rn(2.0 * 3.14159265358979323846, __dsub_rn(xmax, xmin));
+        const int shifted = (2 * j < n) ? j : j - n;
+        const double k = __dmul_rn(dk, (double)shifted);
+        kv[j] = k;
+        kd[j] = cis_minus_one(theta_k(__dmul_rn(k, k), mass, dt));
+    }
+}
+
+template <typename T>
+__global__ void build_twiddles(int n, cx<T>* tw) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        double s, c;
+        sincospi(-2.0 * (double)t / (double)n, &s, &c);
+        tw[t] = mk<T>((T)c, (T)s);
+    }
+}
+
+// Full-N reference tables (propagator-tables surface).
+__global__ void build_full_tables(const double* __restrict__ V, const double* __restrict__ kvx,
+                                  const double* __restrict__ kvy, const double* __restrict__ kvz,
+                                  int nx, int ny, long long N, double dt, double mass,
+                                  cx<double>* half_v, cx<double>* kin) {
+    for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < N;
+         f += (long long)gridDim.x * blockDim.x) {
+        double s, c;
+        if (half_v) {
+            sincos(theta_v(V[f], dt), &s, &c);
+            half_v[f] = mk<double>(c, s);
+        }
+        if (kin) {
+            const long long line = f / nx;
+            const int i = (int)(f - line * nx);
+            const long long k = line / ny;
+            const int j = (int)(line - k * ny);
+            const double a = kvx[i], b = kvy[j], cz = kvz[k];
+            const double ksq = __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(cz, cz));
+            sincos(theta_k(ksq, mass, dt), &s, &c);
+            kin[f] = mk<double>(c, s);
+        }
+    }
+}
+
+}  // namespace sesk

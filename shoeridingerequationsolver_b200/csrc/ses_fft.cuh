@@ -85,8 +85,48 @@ __device__ __forceinline__ uint32_t fdiv(uint32_t x, const FastDiv& f) {
 
 // ---------------------------------------------------------------------------
 // In-register DFTs of size R, forward (e^{-}), natural-order output.
-// The constants are cos/sin of the R-th roots of unity.
+// The constants are cos/sin of the R-th roots of unity.  In FP32 each constant
+// is carried as hi + lo (lo = the FP32 rounding of its remainder) and applied
+// with one extra FMA: a plain FP32 constant such as (float)(1/sqrt 2) is
+// ~1.7e-8 small, and that bias would shrink the norm by ~1e-7 every step.
 // ---------------------------------------------------------------------------
+template <typename T>
+struct CK {
+    T hi, lo;
+};
+
+template <typename T>
+__device__ __forceinline__ CK<T> ck(double c) {
+    if constexpr (sizeof(T) == 4) {
+        const float hi = (float)c;
+        return CK<T>{hi, (float)(c - (double)hi)};
+    } else {
+        return CK<T>{c, 0.0};
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T kmul(T a, CK<T> c) {
+    if constexpr (sizeof(T) == 4) return fmaf(a, c.hi, a * c.lo);
+    else return a * c.hi;
+}
+
+// v * (c - i s) with compensated constants
+template <typename T>
+__device__ __forceinline__ cx<T> rotc(cx<T> v, CK<T> c, CK<T> s) {
+    if constexpr (sizeof(T) == 4) {
+        return mk<T>(fmaf(v.x, c.hi, fmaf(v.y, s.hi, fmaf(v.x, c.lo, v.y * s.lo))),
+                     fmaf(v.y, c.hi, fmaf(-v.x, s.hi, fmaf(v.y, c.lo, -v.x * s.lo))));
+    } else {
+        return mk<T>(v.x * c.hi + v.y * s.hi, v.y * c.hi - v.x * s.hi);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ CK<T> neg(CK<T> c) {
+    return CK<T>{-c.hi, -c.lo};
+}
+
 template <typename T>
 __device__ __forceinline__ void dft2(cx<T>* v) {
     const cx<T> a = v[0];
@@ -106,14 +146,14 @@ __device__ __forceinline__ void dft4(cx<T>* v) {
 
 template <typename T>
 __device__ __forceinline__ void dft8(cx<T>* v) {
-    const T h = (T)0.70710678118654752440;
+    const CK<T> h = ck<T>(0.70710678118654752440);  // cos(pi/4)
     cx<T> e[4] = {v[0], v[2], v[4], v[6]};
     cx<T> o[4] = {v[1], v[3], v[5], v[7]};
     dft4(e);
     dft4(o);
-    o[1] = mk<T>((o[1].x + o[1].y) * h, (o[1].y - o[1].x) * h);   // * e^{-i pi/4}
-    o[2] = mul_mi(o[2]);                                          // * e^{-i pi/2}
-    o[3] = mk<T>((o[3].y - o[3].x) * h, -(o[3].x + o[3].y) * h);  // * e^{-3i pi/4}
+    o[1] = rotc(o[1], h, h);          // * e^{-i pi/4}
+    o[2] = mul_mi(o[2]);              // * e^{-i pi/2}
+    o[3] = rotc(o[3], neg(h), h);     // * e^{-3i pi/4}
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         v[k] = e[k] + o[k];
@@ -123,9 +163,9 @@ __device__ __forceinline__ void dft8(cx<T>* v) {
 
 template <typename T>
 __device__ __forceinline__ void dft16(cx<T>* v) {
-    const T c1 = (T)0.92387953251128675613;  // cos(pi/8)
-    const T s1 = (T)0.38268343236508977173;  // sin(pi/8)
-    const T h = (T)0.70710678118654752440;   // cos(pi/4)
+    const CK<T> c1 = ck<T>(0.92387953251128675613);  // cos(pi/8)
+    const CK<T> s1 = ck<T>(0.38268343236508977173);  // sin(pi/8)
+    const CK<T> h = ck<T>(0.70710678118654752440);   // cos(pi/4)
     cx<T> e[8], o[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -135,13 +175,13 @@ __device__ __forceinline__ void dft16(cx<T>* v) {
     dft8(e);
     dft8(o);
     // o[k] *= e^{-2 pi i k / 16}
-    o[1] = o[1] * mk<T>(c1, -s1);
-    o[2] = mk<T>((o[2].x + o[2].y) * h, (o[2].y - o[2].x) * h);
-    o[3] = o[3] * mk<T>(s1, -c1);
+    o[1] = rotc(o[1], c1, s1);
+    o[2] = rotc(o[2], h, h);
+    o[3] = rotc(o[3], s1, c1);
     o[4] = mul_mi(o[4]);
-    o[5] = o[5] * mk<T>(-s1, -c1);
-    o[6] = mk<T>((o[6].y - o[6].x) * h, -(o[6].x + o[6].y) * h);
-    o[7] = o[7] * mk<T>(-c1, -s1);
+    o[5] = rotc(o[5], neg(s1), c1);
+    o[6] = rotc(o[6], neg(h), h);
+    o[7] = rotc(o[7], neg(c1), s1);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         v[k] = e[k] + o[k];
@@ -151,10 +191,11 @@ __device__ __forceinline__ void dft16(cx<T>* v) {
 
 template <typename T>
 __device__ __forceinline__ void dft3(cx<T>* v) {
-    const T hs3 = (T)0.86602540378443864676;  // sin(2 pi/3)
+    const CK<T> hs3 = ck<T>(0.86602540378443864676);  // sin(2 pi/3)
     const cx<T> t = v[1] + v[2];
     const cx<T> m = mk<T>(v[0].x - (T)0.5 * t.x, v[0].y - (T)0.5 * t.y);
-    const cx<T> d = scale(v[1] - v[2], hs3);
+    const cx<T> df = v[1] - v[2];
+    const cx<T> d = mk<T>(kmul(df.x, hs3), kmul(df.y, hs3));
     v[0] = v[0] + t;
     v[1] = mk<T>(m.x + d.y, m.y - d.x);  // m - i d
     v[2] = mk<T>(m.x - d.y, m.y + d.x);  // m + i d
@@ -162,16 +203,16 @@ __device__ __forceinline__ void dft3(cx<T>* v) {
 
 template <typename T>
 __device__ __forceinline__ void dft5(cx<T>* v) {
-    const T c1 = (T)0.30901699437494742410;   // cos(2 pi/5)
-    const T c2 = (T)-0.80901699437494742410;  // cos(4 pi/5)
-    const T s1 = (T)0.95105651629515357212;   // sin(2 pi/5)
-    const T s2 = (T)0.58778525229247312917;   // sin(4 pi/5)
+    const CK<T> c1 = ck<T>(0.30901699437494742410);   // cos(2 pi/5)
+    const CK<T> c2 = ck<T>(-0.80901699437494742410);  // cos(4 pi/5)
+    const CK<T> s1 = ck<T>(0.95105651629515357212);   // sin(2 pi/5)
+    const CK<T> s2 = ck<T>(0.58778525229247312917);   // sin(4 pi/5)
     const cx<T> a1 = v[1] + v[4], a2 = v[2] + v[3];
     const cx<T> b1 = v[1] - v[4], b2 = v[2] - v[3];
-    const cx<T> p1 = mk<T>(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
-    const cx<T> p2 = mk<T>(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
-    const cx<T> q1 = mk<T>(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y);
-    const cx<T> q2 = mk<T>(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y);
+    const cx<T> p1 = mk<T>(v[0].x + kmul(a1.x, c1) + kmul(a2.x, c2), v[0].y + kmul(a1.y, c1) + kmul(a2.y, c2));
+    const cx<T> p2 = mk<T>(v[0].x + kmul(a1.x, c2) + kmul(a2.x, c1), v[0].y + kmul(a1.y, c2) + kmul(a2.y, c1));
+    const cx<T> q1 = mk<T>(kmul(b1.x, s1) + kmul(b2.x, s2), kmul(b1.y, s1) + kmul(b2.y, s2));
+    const cx<T> q2 = mk<T>(kmul(b1.x, s2) - kmul(b2.x, s1), kmul(b1.y, s2) - kmul(b2.y, s1));
     v[0] = v[0] + a1 + a2;
     v[1] = mk<T>(p1.x + q1.y, p1.y - q1.x);  // p1 - i q1
     v[4] = mk<T>(p1.x - q1.y, p1.y + q1.x);  // p1 + i q1

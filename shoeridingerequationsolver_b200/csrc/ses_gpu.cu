@@ -12,8 +12,12 @@
 #include <thread>
 #include <vector>
 
+#include <mutex>
+
 #include "ses_gpu.h"
+#include "ses_aux.cuh"
 #include "ses_pass.cuh"
+#include "ses_plans.cuh"
 
 using namespace sesk;
 
@@ -68,7 +72,68 @@ struct PassPlan {
     unsigned grid = 0;
     long long nlines = 0;
     long long nu = 0, sw = 0, se = 0;
+    // compiled plan (nullptr: run-time plan kernels)
+    const void* cp = nullptr;
+    unsigned cgrid = 0, cblock = 0;
+    size_t csmem = 0;
 };
+
+struct Registry {
+    std::vector<PlanEntry<float>> f;
+    std::vector<PlanEntry<double>> d;
+};
+
+const Registry& registry() {
+    static Registry r;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        register_plans_small(r.f, r.d);
+        register_plans_mixed(r.f, r.d);
+        register_plans_256(r.f, r.d);
+        register_plans_large(r.f, r.d);
+    });
+    return r;
+}
+
+template <typename T>
+const PlanEntry<T>* find_plan(int n) {
+    const auto& v = [] () -> const std::vector<PlanEntry<T>>& {
+        if constexpr (sizeof(T) == 4) return registry().f;
+        else return registry().d;
+    }();
+    for (const auto& e : v)
+        if (e.n == n) return &e;
+    return nullptr;
+}
+
+// Per-stage twiddles of a compiled plan, forward order then reversed order:
+// stage (R, Ns) holds w^{r k N/(Ns R)} at [r*Ns + k], w = e^{-2 pi i/N}, in FP64.
+std::vector<double> stage_twiddles(int n, int r0, int r1, int r2) {
+    std::vector<double> out;
+    auto add_plan = [&](const int* rad, int cnt) {
+        int Ns = 1;
+        for (int p = 0; p < cnt; ++p) {
+            const int R = rad[p];
+            for (int r = 0; r < R; ++r)
+                for (int k = 0; k < Ns; ++k) {
+                    const long long e = ((long long)r * k * (n / (Ns * R))) % n;
+                    const double th = -2.0 * 3.14159265358979323846 * (double)e / (double)n;
+                    out.push_back(std::cos(th));
+                    out.push_back(std::sin(th));
+                }
+            Ns *= R;
+        }
+    };
+    int fwd[3], cnt = 0;
+    for (int r : {r0, r1, r2})
+        if (r > 1) fwd[cnt++] = r;
+    if (cnt == 0) fwd[cnt++] = 1;
+    int rev[3];
+    for (int i = 0; i < cnt; ++i) rev[i] = fwd[cnt - 1 - i];
+    add_plan(fwd, cnt);
+    add_plan(rev, cnt);
+    return out;
+}
 
 int threads_for(int L, int n, const std::vector<int>& rad) {
     int t = 32;
@@ -161,6 +226,8 @@ struct ses_solver {
     bool has_mask = false;
 
     PassPlan pp[3];
+    void* stw[3] = {nullptr, nullptr, nullptr};   // compiled-plan stage twiddles (hi)
+    void* stwl[3] = {nullptr, nullptr, nullptr};  // FP32 remainders (lo)
     int last_axis = 0;  // highest axis with n > 1 (0 for 1D / single point)
 
     double* partials = nullptr;
@@ -205,6 +272,8 @@ void release(ses_solver* h) {
         if (h->kv[a]) cudaFree(h->kv[a]);
         if (h->kd[a]) cudaFree(h->kd[a]);
         if (h->mask1[a]) cudaFree(h->mask1[a]);
+        if (h->stw[a]) cudaFree(h->stw[a]);
+        if (h->stwl[a]) cudaFree(h->stwl[a]);
     }
     if (h->hsums) cudaFreeHost(h->hsums);
     if (h->ev) cudaEventDestroy(h->ev);
@@ -266,6 +335,8 @@ PassArgs<T> make_args(const ses_solver* h, int axis, const void* src, void* dst)
     a.fny = make_fastdiv((uint32_t)ny);
     a.fnx = make_fastdiv((uint32_t)nx);
     a.tw = reinterpret_cast<const cx<T>*>(h->tw[axis]);
+    a.stw = reinterpret_cast<const cx<T>*>(h->stw[axis]);
+    a.stwl = reinterpret_cast<const cx<T>*>(h->stwl[axis]);
     a.out_scale = 1.0;
     Tables& tb = a.tb;
     tb.vtab = h->vtab;
@@ -310,8 +381,14 @@ XKernel<T> skernel(int mode) {
 template <typename T>
 ses_status launch(const ses_solver* h, int axis, int mode, const PassArgs<T>& a, cudaStream_t s) {
     const PassPlan& pp = h->pp[axis];
-    XKernel<T> k = axis == 0 ? xkernel<T>(mode) : skernel<T>(mode);
-    k<<<pp.grid, pp.g.nthreads, pp.smem, s>>>(a);
+    if (pp.cp) {
+        const PlanEntry<T>* e = reinterpret_cast<const PlanEntry<T>*>(pp.cp);
+        PassKernel<T> k = axis == 0 ? e->xk[mode] : e->sk[mode];
+        k<<<pp.cgrid, pp.cblock, pp.csmem, s>>>(a);
+    } else {
+        XKernel<T> k = axis == 0 ? xkernel<T>(mode) : skernel<T>(mode);
+        k<<<pp.grid, pp.g.nthreads, pp.smem, s>>>(a);
+    }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return fail(SES_EDEVICE, std::string("pass launch: ") + cudaGetErrorString(e));
@@ -508,7 +585,7 @@ ses_status enqueue_observe(ses_solver* h, double xlo, double xhi) {
         XProg p;
         p.mode = XM_REDUCE;
         SES_TRY(pass_x<T>(h, h->psi, h->scratch, p, s));
-        rows = h->pp[0].grid;
+        rows = h->pp[0].cp ? h->pp[0].cgrid : h->pp[0].grid;
     } else {
         XProg p;
         p.mode = XM_FWD;
@@ -516,7 +593,7 @@ ses_status enqueue_observe(ses_solver* h, double xlo, double xhi) {
         if (h->last_axis == 2 && h->n[1] > 1)
             SES_TRY(pass_s<T>(h, 1, h->scratch, h->scratch, SM_FWD, 1.0, s));
         SES_TRY(pass_s<T>(h, h->last_axis, h->scratch, h->scratch, SM_REDUCE, 1.0, s));
-        rows = h->pp[h->last_axis].grid;
+        rows = h->pp[h->last_axis].cp ? h->pp[h->last_axis].cgrid : h->pp[h->last_axis].grid;
     }
     finalize_kernel<<<1, 32, 0, s>>>(h->partials, (int)rows, kRedK, h->dsums + kRedR);
     SES_CU(cudaGetLastError());
@@ -641,6 +718,71 @@ ses_status build_tables(ses_solver* h) {
     return SES_OK;
 }
 
+void attach_compiled_plan(ses_solver* h, int axis) {
+    PassPlan& pp = h->pp[axis];
+    const int n = h->n[axis];
+    pp.cp = nullptr;
+    if (n < 2) return;
+    int e = 0, ls = 0, xw = 4;
+    if (h->prec == SES_C128) {
+        if (const PlanEntry<double>* p = find_plan<double>(n)) {
+            pp.cp = p;
+            e = p->e;
+            ls = p->ls;
+            xw = p->xw;
+        }
+    } else if (const PlanEntry<float>* p = find_plan<float>(n)) {
+        pp.cp = p;
+        e = p->e;
+        ls = p->ls;
+        xw = p->xw;
+    }
+    if (!pp.cp) return;
+    const int tl = n / e;
+    if (axis == 0) {
+        const long long lpc = (long long)xw * (32 / tl);
+        pp.cgrid = (unsigned)((pp.nlines + lpc - 1) / lpc);
+        pp.cblock = 32 * xw;
+        pp.csmem = 0;
+    } else {
+        pp.cgrid = (unsigned)((pp.nlines + ls - 1) / ls);
+        pp.cblock = (unsigned)(ls * tl);
+        pp.csmem = (size_t)n * ls * h->esize;
+    }
+}
+
+ses_status upload_stage_twiddles(ses_solver* h) {
+    for (int a = 0; a < 3; ++a) {
+        const PassPlan& pp = h->pp[a];
+        if (!pp.cp) continue;
+        int r0, r1, r2;
+        if (h->prec == SES_C128) {
+            const auto* p = reinterpret_cast<const PlanEntry<double>*>(pp.cp);
+            r0 = p->r0; r1 = p->r1; r2 = p->r2;
+        } else {
+            const auto* p = reinterpret_cast<const PlanEntry<float>*>(pp.cp);
+            r0 = p->r0; r1 = p->r1; r2 = p->r2;
+        }
+        const std::vector<double> t = stage_twiddles(h->n[a], r0, r1, r2);
+        const size_t cnt = t.size() / 2;
+        if (h->prec == SES_C128) {
+            SES_TRY(dalloc(h, &h->stw[a], cnt * sizeof(cx<double>)));
+            SES_CU(cudaMemcpy(h->stw[a], t.data(), cnt * sizeof(cx<double>), cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> hi(2 * cnt), lo(2 * cnt);
+            for (size_t i = 0; i < 2 * cnt; ++i) {
+                hi[i] = (float)t[i];
+                lo[i] = (float)(t[i] - (double)hi[i]);
+            }
+            SES_TRY(dalloc(h, &h->stw[a], cnt * sizeof(cx<float>)));
+            SES_TRY(dalloc(h, &h->stwl[a], cnt * sizeof(cx<float>)));
+            SES_CU(cudaMemcpy(h->stw[a], hi.data(), cnt * sizeof(cx<float>), cudaMemcpyHostToDevice));
+            SES_CU(cudaMemcpy(h->stwl[a], lo.data(), cnt * sizeof(cx<float>), cudaMemcpyHostToDevice));
+        }
+    }
+    return SES_OK;
+}
+
 ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt, double mass,
                        const double* V, const double* psi0, bool with_tables, ses_handle* out) {
     if (!grid || !out) return fail(SES_EINVAL, "null grid or output pointer");
@@ -687,6 +829,8 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
         if (!plan_pass(h->n[a], h->esize, a != 0, nlines[a], h->pp[a], why))
             return bail(fail(SES_EINVAL, why));
         rows = std::max<size_t>(rows, h->pp[a].grid);
+        attach_compiled_plan(h, a);
+        rows = std::max<size_t>(rows, h->pp[a].cgrid);
     }
     if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev, cudaEventDisableTiming) != cudaSuccess) {
@@ -722,6 +866,7 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
                                                      with_tables ? mass : 1.0, h->kv[a], h->kd[a]);
     }
     if (cudaGetLastError() != cudaSuccess) return bail(fail(SES_EDEVICE, "axis table build failed"));
+    if ((st = upload_stage_twiddles(h)) != SES_OK) return bail(st);
     if (with_tables) {
         if ((st = dalloc(h, (void**)&h->V, N * sizeof(double))) != SES_OK) return bail(st);
         if ((st = dalloc(h, &h->vtab, N * h->esize)) != SES_OK) return bail(st);

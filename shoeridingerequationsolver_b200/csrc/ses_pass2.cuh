@@ -1,0 +1,359 @@
+// Compiled-plan axis passes: the line FFT of length N = R0*R1*R2 runs with
+// each thread holding E elements of its line in registers.  Butterfly j of a
+// stage belongs to thread q = j mod (N/E); between stages the elements are
+// exchanged through shared memory.  On the contiguous x axis a line lives
+// inside one warp (exchange = __syncwarp); on the strided y/z axes consecutive
+// threads own consecutive lines (coalesced) and exchanges are CTA-wide.
+//
+// The last stage of an FFT leaves thread q holding positions
+// q + (N/E) b + r N/R_last, exactly the inputs the FIRST stage of an FFT with
+// the reversed radix order needs, so the two FFTs of a fused pass (inverse
+// then forward, or forward then inverse) run back to back in registers.
+#pragma once
+
+#include "ses_pass.cuh"
+
+namespace sesk {
+
+template <typename T>
+__device__ __forceinline__ cx<T> twmul(cx<T> v, const cx<T>* __restrict__ hi,
+                                       const cx<T>* __restrict__ lo, int idx) {
+    const cx<T> h = hi[idx];
+    if constexpr (sizeof(T) == 4) {  // compensated: v * (h + l), l = FP32 remainder of the FP64 twiddle
+        const cx<T> l = lo[idx];
+        return mk<T>(fmaf(v.x, h.x, fmaf(-v.y, h.y, fmaf(v.x, l.x, -v.y * l.y))),
+                     fmaf(v.x, h.y, fmaf(v.y, h.x, fmaf(v.x, l.y, v.y * l.x))));
+    } else {
+        return v * h;
+    }
+}
+
+// Offset of stage p's table: tables are R_p x Ns_p entries, w^{r k N/(Ns R)} at [r*Ns + k].
+template <int R0, int R1, int R2>
+struct StageOff {
+    static constexpr int o0 = 0;
+    static constexpr int o1 = R0 * 1;
+    static constexpr int o2 = o1 + R1 * R0;
+};
+
+template <typename T, int N, int E, int TL, int R, int NS, int OFF>
+__device__ __forceinline__ void rstage(cx<T> (&v)[E], int q, const cx<T>* __restrict__ twh,
+                                       const cx<T>* __restrict__ twl) {
+    constexpr int B = E / R;
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        if constexpr (NS > 1) {
+            const int k = (q + TL * b) % NS;
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[b * R + r] = twmul(v[b * R + r], twh, twl, OFF + r * NS + k);
+        }
+        dft<T, R>(&v[b * R]);
+    }
+}
+
+template <typename T, int N, int E, int TL, int RP, int NSP, int RN, class X>
+__device__ __forceinline__ void rexchange(cx<T> (&v)[E], int q, X& x) {
+#pragma unroll
+    for (int b = 0; b < E / RP; ++b) {
+        const int j = q + TL * b;
+        const int k = j % NSP;
+        const int base = (j - k) * RP + k;
+#pragma unroll
+        for (int r = 0; r < RP; ++r) x.put(base + r * NSP, v[b * RP + r]);
+    }
+    x.sync();
+#pragma unroll
+    for (int b = 0; b < E / RN; ++b) {
+        const int j = q + TL * b;
+#pragma unroll
+        for (int r = 0; r < RN; ++r) v[b * RN + r] = x.get(j + r * (N / RN));
+    }
+    x.sync();
+}
+
+// Forward FFT of plan (R0, R1, R2) (R = 1: stage absent), tables of that plan.
+// In:  v[b*R0 + r] = x[q + TL b + r N/R0].   Out: v[b*RL + r] = X[q + TL b + r N/RL].
+template <typename T, int N, int E, int R0, int R1, int R2, int TOFF, class X>
+__device__ __forceinline__ void rfft(cx<T> (&v)[E], int q, const cx<T>* twh, const cx<T>* twl, X& x) {
+    constexpr int TL = N / E;
+    rstage<T, N, E, TL, R0, 1, TOFF>(v, q, twh, twl);
+    if constexpr (R1 > 1) {
+        rexchange<T, N, E, TL, R0, 1, R1>(v, q, x);
+        rstage<T, N, E, TL, R1, R0, TOFF + R0>(v, q, twh, twl);
+    }
+    if constexpr (R2 > 1) {
+        rexchange<T, N, E, TL, R1, R0, R2>(v, q, x);
+        rstage<T, N, E, TL, R2, R0 * R1, TOFF + R0 + R1 * R0>(v, q, twh, twl);
+    }
+}
+
+template <int R0, int R1, int R2>
+struct PlanShape {
+    static constexpr int last = R2 > 1 ? R2 : (R1 > 1 ? R1 : R0);
+    // reversed order (R2, R1, R0) without absent stages
+    static constexpr int v0 = R2 > 1 ? R2 : (R1 > 1 ? R1 : R0);
+    static constexpr int v1 = R2 > 1 ? R1 : (R1 > 1 ? R0 : 1);
+    static constexpr int v2 = R2 > 1 ? R0 : 1;
+    static constexpr int fwd_tables = R0 + (R1 > 1 ? R1 * R0 : 0) + (R2 > 1 ? R2 * R0 * R1 : 0);
+};
+
+// FFT with the plan's own order (tables at 0) or reversed order (tables after).
+template <typename T, int N, int E, int R0, int R1, int R2, bool REV, class X>
+__device__ __forceinline__ void rfft_plan(cx<T> (&v)[E], int q, const cx<T>* twh, const cx<T>* twl,
+                                          X& x) {
+    using S = PlanShape<R0, R1, R2>;
+    if constexpr (!REV) rfft<T, N, E, R0, R1, R2, 0>(v, q, twh, twl, x);
+    else rfft<T, N, E, S::v0, S::v1, S::v2, S::fwd_tables>(v, q, twh, twl, x);
+}
+
+template <typename T, int PITCH>
+struct XchWarp {
+    cx<T>* p;
+    __device__ __forceinline__ void put(int pos, cx<T> v) { p[pos + (pos >> 4)] = v; }
+    __device__ __forceinline__ cx<T> get(int pos) const { return p[pos + (pos >> 4)]; }
+    __device__ __forceinline__ void sync() { __syncwarp(); }
+};
+
+template <typename T, int L>
+struct XchCta {
+    cx<T>* p;
+    int l;
+    __device__ __forceinline__ void put(int pos, cx<T> v) { p[pos * L + l] = v; }
+    __device__ __forceinline__ cx<T> get(int pos) const { return p[pos * L + l]; }
+    __device__ __forceinline__ void sync() { __syncthreads(); }
+};
+
+template <typename T>
+__device__ __forceinline__ cx<T> czero() {
+    return mk<T>((T)0, (T)0);
+}
+
+// ---------------------------------------------------------------------------
+// Contiguous-axis (x) pass, compiled plan.  4 warps per CTA; a warp owns
+// 32/(N/E) lines.  Modes as in XMode.
+// ---------------------------------------------------------------------------
+// Warps per contiguous-pass CTA: up to 4, within 48 KB of static shared memory.
+template <typename T, int N, int E>
+struct XShape {
+    static constexpr int TL = N / E;
+    static constexpr int LPW = 32 / TL;          // lines per warp
+    static constexpr int PITCH = N + N / 16;     // one pad element every 16
+    static constexpr int per_warp = LPW * PITCH * (int)sizeof(cx<T>);
+    static constexpr int NW = (48 * 1024) / per_warp >= 4 ? 4 : ((48 * 1024) / per_warp < 1 ? 1 : (48 * 1024) / per_warp);
+};
+
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2>
+__global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4) xpass2_kernel(const PassArgs<T> a) {
+    using XS = XShape<T, N, E>;
+    constexpr int TL = XS::TL;
+    constexpr int LPW = XS::LPW;
+    constexpr int PITCH = XS::PITCH;
+    constexpr int NW = XS::NW;
+    using S = PlanShape<R0, R1, R2>;
+    constexpr int RF = R0, RL = S::last;
+    __shared__ cx<T> xb[NW * LPW * PITCH];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lw = lane / TL, q = lane % TL;
+    const long long m = ((long long)blockIdx.x * NW + warp) * LPW + lw;
+    const bool valid = m < a.nlines;
+    const long long mc = valid ? m : 0;
+    const int kz = (int)fdiv((uint32_t)mc, a.fny);
+    const int jy = (int)(mc - (long long)kz * a.ny);
+    XchWarp<T, PITCH> x{xb + (warp * LPW + lw) * PITCH};
+    const cx<T>* src = a.src + mc * N;
+    cx<T>* dst = a.dst + mc * N;
+    cx<T> v[E];
+
+    // load the first FFT's inputs (coalesced along the line)
+    constexpr bool kConjIn = MODE == XM_INV || MODE == XM_MID || MODE == XM_END;
+#pragma unroll
+    for (int b = 0; b < E / RF; ++b)
+#pragma unroll
+        for (int r = 0; r < RF; ++r) {
+            const int pos = q + TL * b + r * (N / RF);
+            cx<T> e = valid ? src[pos] : czero<T>();
+            if constexpr (MODE == XM_START || MODE == XM_1D) {
+                if (a.d_load != DG_NONE || a.m_load)
+                    e = apply_diag(e, a.d_load, a.m_load, mc * N + pos, pos, jy, kz, a.tb);
+            }
+            v[b * RF + r] = kConjIn ? cconj(e) : e;
+        }
+
+    rfft_plan<T, N, E, R0, R1, R2, false>(v, q, a.stw, a.stwl, x);
+    // v[b*RL + r] now at position q + TL b + r N/RL
+
+    if constexpr (MODE == XM_REDUCE) {
+        double acc[kRedK] = {0, 0, 0, 0, 0};
+        if (valid) {
+#pragma unroll
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const int pos = q + TL * b + r * (N / RL);
+                    const double k3[3] = {a.tb.kv[0][pos], a.tb.kv[1][jy], a.tb.kv[2][kz]};
+                    const cx<double> p = widen(v[b * RL + r]);
+                    acc_k(acc, p.x * p.x + p.y * p.y, k3, a.tb.inv_mass);
+                }
+        }
+        block_reduce_store<kRedK>(acc, a.partials);
+        return;
+    }
+    if constexpr (MODE == XM_FWD || MODE == XM_START || MODE == XM_INV || MODE == XM_END) {
+        const T sc = (T)a.out_scale;
+        if (valid) {
+#pragma unroll
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const int pos = q + TL * b + r * (N / RL);
+                    cx<T> e = v[b * RL + r];
+                    if constexpr (MODE == XM_INV) e = scale(cconj(e), sc);
+                    if constexpr (MODE == XM_END) {
+                        e = cconj(e);
+                        if (a.d_store != DG_NONE || a.m_store)
+                            e = apply_diag(e, a.d_store, a.m_store, mc * N + pos, pos, jy, kz, a.tb);
+                    }
+                    dst[pos] = e;
+                }
+        }
+        return;
+    }
+    if constexpr (MODE == XM_MID || MODE == XM_1D) {
+        // between the FFTs: MID -> conj, V (* M) in real space; 1D -> K/N, conj
+        const cx<double> dyz = dmul1(a.tb.kd[1][jy], a.tb.kd[2][kz]);
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int pos = q + TL * b + r * (N / RL);
+                cx<T> e = v[b * RL + r];
+                if constexpr (MODE == XM_MID) {
+                    e = cconj(e);
+                    if (a.d_mid != DG_NONE || a.m_mid)
+                        e = apply_diag(e, a.d_mid, a.m_mid, mc * N + pos, pos, jy, kz, a.tb);
+                } else {
+                    e = kinetic_conj(e, dmul1(dyz, a.tb.kd[0][pos]), a.tb.kscale);
+                }
+                v[b * RL + r] = e;
+            }
+        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+        // v[b*R0 + r] at position q + TL b + r N/R0
+        if (valid) {
+#pragma unroll
+            for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                for (int r = 0; r < R0; ++r) {
+                    const int pos = q + TL * b + r * (N / R0);
+                    cx<T> e = v[b * R0 + r];
+                    if constexpr (MODE == XM_1D) {
+                        e = cconj(e);
+                        if (a.d_store != DG_NONE || a.m_store)
+                            e = apply_diag(e, a.d_store, a.m_store, mc * N + pos, pos, jy, kz, a.tb);
+                    }
+                    dst[pos] = e;
+                }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Strided-axis (y or z) pass, compiled plan.  CTA = L lines x N/E threads per
+// line; thread (l = tid % L, q = tid / L).  Modes as in SModeK.
+// ---------------------------------------------------------------------------
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L>
+__global__ void __launch_bounds__(L*(N / E), 1) spass2_kernel(const PassArgs<T> a) {
+    constexpr int TL = N / E;
+    using S = PlanShape<R0, R1, R2>;
+    constexpr int RL = S::last;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T>* tile = reinterpret_cast<cx<T>*>(smraw);
+    const int l = threadIdx.x % L, q = threadIdx.x / L;
+    const long long s = (long long)blockIdx.x * L + l;
+    const bool valid = s < a.nlines;
+    const long long sc_ = valid ? s : 0;
+    const long long w = (long long)fdiv((uint32_t)sc_, a.fnu);
+    const long long u = sc_ - w * a.nu;
+    const long long base = u + w * a.sw;
+    const long long se = a.se;
+    XchCta<T, L> x{tile, l};
+    cx<T> v[E];
+    constexpr bool kConjIn = MODE == SM_INV;
+#pragma unroll
+    for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const int pos = q + TL * b + r * (N / R0);
+            const cx<T> e = valid ? a.src[base + pos * se] : czero<T>();
+            v[b * R0 + r] = kConjIn ? cconj(e) : e;
+        }
+
+    rfft_plan<T, N, E, R0, R1, R2, false>(v, q, a.stw, a.stwl, x);
+
+    const bool ypass = a.axis == 1;
+    int c1, c2;  // the line's other two coordinates: y-pass (x, z), z-pass (x, y)
+    if (ypass) {
+        c1 = (int)u;
+        c2 = (int)w;
+    } else {
+        c2 = (int)fdiv((uint32_t)u, a.fnx);
+        c1 = (int)(u - (long long)c2 * a.nx);
+    }
+
+    if constexpr (MODE == SM_REDUCE) {
+        double acc[kRedK] = {0, 0, 0, 0, 0};
+        if (valid) {
+            const double* kva = ypass ? a.tb.kv[1] : a.tb.kv[2];
+            const double k1 = a.tb.kv[0][c1], k2 = ypass ? a.tb.kv[2][c2] : a.tb.kv[1][c2];
+#pragma unroll
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const int pos = q + TL * b + r * (N / RL);
+                    const double ka = kva[pos];
+                    const double k3[3] = {k1, ypass ? ka : k2, ypass ? k2 : ka};
+                    const cx<double> p = widen(v[b * RL + r]);
+                    acc_k(acc, p.x * p.x + p.y * p.y, k3, a.tb.inv_mass);
+                }
+        }
+        block_reduce_store<kRedK>(acc, a.partials);
+        return;
+    }
+    if constexpr (MODE == SM_FWD || MODE == SM_INV) {
+        const T scl = (T)a.out_scale;
+        if (valid) {
+#pragma unroll
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const int pos = q + TL * b + r * (N / RL);
+                    cx<T> e = v[b * RL + r];
+                    if constexpr (MODE == SM_INV) e = scale(cconj(e), scl);
+                    a.dst[base + pos * se] = e;
+                }
+        }
+        return;
+    }
+    if constexpr (MODE == SM_FUSED) {
+        const cx<double> dother = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
+        const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int pos = q + TL * b + r * (N / RL);
+                v[b * RL + r] = kinetic_conj(v[b * RL + r], dmul1(dother, kda[pos]), a.tb.kscale);
+            }
+        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+        if (valid) {
+#pragma unroll
+            for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                for (int r = 0; r < R0; ++r) {
+                    const int pos = q + TL * b + r * (N / R0);
+                    a.dst[base + pos * se] = cconj(v[b * R0 + r]);
+                }
+        }
+    }
+}
+
+}  // namespace sesk

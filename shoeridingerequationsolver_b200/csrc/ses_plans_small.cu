@@ -1,0 +1,15 @@
+// Compiled plans: 16, 32, 64, 128.
+#include "ses_plans.cuh"
+
+namespace sesk {
+void register_plans_small(std::vector<PlanEntry<float>>& f, std::vector<PlanEntry<double>>& d) {
+    f.push_back(make_plan_entry<float, 16, 16, 16, 1, 1, 32>());
+    d.push_back(make_plan_entry<double, 16, 16, 16, 1, 1, 16>());
+    f.push_back(make_plan_entry<float, 32, 8, 8, 4, 1, 32>());
+    d.push_back(make_plan_entry<double, 32, 8, 8, 4, 1, 16>());
+    f.push_back(make_plan_entry<float, 64, 8, 8, 8, 1, 32>());
+    d.push_back(make_plan_entry<double, 64, 8, 8, 8, 1, 16>());
+    f.push_back(make_plan_entry<float, 128, 16, 16, 8, 1, 32>());
+    d.push_back(make_plan_entry<double, 128, 16, 16, 8, 1, 16>());
+}
+}  // namespace sesk

@@ -1,0 +1,117 @@
+// C++ caller of the B200 path through include/ses_gpu.hpp, written the way the
+// reference's own gtest cases use ses::SplitOperator3D / ses::fft (reference
+// tests/fft3_test.cpp, propagator_tables_test.cpp, solver/src/vkcheck_main.cpp
+// check_engine_step), checked against the FP64 oracle (oracle/ses_oracle.h).
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <stdexcept>
+#include <vector>
+
+#include "ses_gpu.hpp"
+#include "ses_oracle.h"
+
+using ses::gpu::cd;
+
+static int failures = 0;
+#define EXPECT(cond, what)                                   \
+    do {                                                     \
+        if (!(cond)) {                                       \
+            std::printf("FAIL %s\n", what);                  \
+            ++failures;                                      \
+        } else {                                             \
+            std::printf("PASS %s\n", what);                  \
+        }                                                    \
+    } while (0)
+
+int main() {
+    const double pi = 3.14159265358979323846;
+    {  // fft3_test.cpp PlaneWaveSpikesAtItsBin
+        const int nx = 8, ny = 16, nz = 4;
+        ses::gpu::Field3D f{ses::gpu::Grid3D{{0, 1, nx}, {0, 1, ny}, {0, 1, nz}}};
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double th = 2 * pi * (3.0 * i / nx + 5.0 * j / ny + 1.0 * k / nz);
+                    f(i, j, k) = cd{std::cos(th), std::sin(th)};
+                }
+        ses::gpu::fft(f);
+        double worst = 0;
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double e = (i == 3 && j == 5 && k == 1) ? 512.0 : 0.0;
+                    worst = std::fmax(worst, std::abs(f(i, j, k) - cd{e, 0}));
+                }
+        EXPECT(worst < 1e-9, "fft3 plane wave spike");
+    }
+    {  // check_engine_step: 8^3 soft Coulomb, dt 0.02, 20 steps vs the FP64 core
+        const double box[6] = {-4, 4, -4, 4, -4, 4};
+        const int n[3] = {8, 8, 8};
+        const double c[3] = {0, 0, 0}, r0[3] = {1, 0, 0}, sg[3] = {1.2, 1.2, 1.2}, k0[3] = {0, 0.5, 0};
+        std::vector<double> V(512);
+        seso_soft_coulomb3d(box, n, 1.0, 1.0, c, V.data());
+        std::vector<cd> psi0(512);
+        seso_gaussian3d(box, n, r0, sg, k0, reinterpret_cast<double*>(psi0.data()));
+        std::vector<cd> ref = psi0;
+        seso_step3d(box, n, V.data(), 0.02, 1.0, nullptr, reinterpret_cast<double*>(ref.data()), 20);
+        const ses::gpu::Grid3D g{{-4, 4, 8}, {-4, 4, 8}, {-4, 4, 8}};
+        for (ses_precision p : {SES_C128, SES_C64}) {
+            ses::gpu::SplitOperator3D prop{g, V, 0.02, 1.0, p};
+            ses::gpu::Field3D f{g};
+            f.data() = psi0;
+            prop.step(f, 20);
+            double num = 0, den = 0;
+            for (std::size_t i = 0; i < ref.size(); ++i) {
+                num += std::norm(f.data()[i] - ref[i]);
+                den += std::norm(ref[i]);
+            }
+            const double err = std::sqrt(num / den);
+            std::printf("  rel L2 (%s) = %.3e\n", p == SES_C128 ? "c128" : "c64", err);
+            EXPECT(err < (p == SES_C128 ? 20e-12 : 1e-5), "engine step vs FP64 core");
+        }
+    }
+    {  // propagator_tables_test.cpp: entries == formula within EXPECT_DOUBLE_EQ (4 ulp)
+        const double box[6] = {0, 4, 0, 4, 0, 4};
+        const int n[3] = {4, 4, 4};
+        const double c[3] = {1, 2, 3};
+        std::vector<double> V(64);
+        seso_harmonic3d(box, n, 2.0, c, V.data());
+        std::vector<cd> half(64), kin(64);
+        seso_tables3d(box, n, V.data(), 0.1, 1.0, reinterpret_cast<double*>(half.data()),
+                      reinterpret_cast<double*>(kin.data()));
+        const ses::gpu::Grid3D g{{0, 4, 4}, {0, 4, 4}, {0, 4, 4}};
+        ses::gpu::SplitOperator3D prop{g, V, 0.1};
+        const auto h = prop.half_potential_phase();
+        const auto k = prop.kinetic_phase();
+        double worst = 0;  // in units of 2^-52 (entries are <= 1 in magnitude)
+        for (int i = 0; i < 64; ++i) {
+            worst = std::fmax(worst, std::fabs(h[i].real() - half[i].real()) / std::ldexp(1.0, -52));
+            worst = std::fmax(worst, std::fabs(h[i].imag() - half[i].imag()) / std::ldexp(1.0, -52));
+            worst = std::fmax(worst, std::fabs(k[i].real() - kin[i].real()) / std::ldexp(1.0, -52));
+            worst = std::fmax(worst, std::fabs(k[i].imag() - kin[i].imag()) / std::ldexp(1.0, -52));
+        }
+        EXPECT(worst <= 4.0, "propagator tables match the formula");
+        EXPECT(prop.dt() == 0.1, "dt accessor");
+    }
+    {  // non-2^a3^b5^c size throws std::invalid_argument, like the reference
+        bool threw = false;
+        try {
+            ses::gpu::SplitOperator3D bad{ses::gpu::Grid3D{{0, 1, 7}, {0, 1, 8}, {0, 1, 8}},
+                                          std::vector<double>(448, 0.0), 0.1};
+        } catch (const std::invalid_argument&) {
+            threw = true;
+        }
+        EXPECT(threw, "unsupported size throws std::invalid_argument");
+    }
+    {  // propagator_test.cpp ConservesNorm (1024 points, dt 0.05, 200 steps)
+        std::vector<cd> psi(1024);
+        seso_gaussian1d(-40, 40, 1024, -15, 1, 2, reinterpret_cast<double*>(psi.data()));
+        ses::gpu::SplitOperator1D prop{ses::gpu::Grid1D{-40, 40, 1024}, std::vector<double>(1024, 0.0), 0.05};
+        prop.step(psi, 200);
+        const double nrm = seso_norm1d(-40, 40, 1024, reinterpret_cast<const double*>(psi.data()));
+        EXPECT(std::fabs(nrm - 1.0) < 1e-12, "1D free packet conserves norm");
+    }
+    std::printf("%s (%d failures)\n", failures ? "FAILED" : "OK", failures);
+    return failures ? 1 : 0;
+}

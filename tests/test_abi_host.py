@@ -194,3 +194,84 @@ def test_plans_stay_in_bounds(dims, es):
             assert (nx - 1) + (nz - 1) * nx * ny + (ny - 1) * nx < N
         else:
             assert (nx * ny - 1) + (nz - 1) * nx * ny < N
+
+
+# ---------------------------------------------------------------------------
+# Compiled plans (ses_pass2.cuh): the register-resident FFT with thread
+# q = j mod (N/E), exchanges through shared memory, per-stage twiddle tables
+# laid out forward-then-reversed, and the reversed-order continuation used by
+# fused passes -- modelled exactly and compared with numpy's FFT.
+
+COMPILED_PLANS = [(16, 16, (16,)), (32, 8, (8, 4)), (48, 12, (4, 4, 3)), (64, 8, (8, 8)),
+                  (96, 24, (8, 4, 3)), (128, 16, (16, 8)), (160, 40, (8, 4, 5)), (256, 16, (16, 16)),
+                  (512, 16, (8, 8, 8)), (1024, 32, (16, 8, 8))]
+
+
+def stage_table(N, rads):
+    """Host table (ses_gpu.cu stage_twiddles): forward order then reversed order."""
+    out = []
+    for order in (rads, tuple(reversed(rads))):
+        Ns = 1
+        for R in order:
+            for r in range(R):
+                for k in range(Ns):
+                    out.append(np.exp(-2j * np.pi * ((r * k * (N // (Ns * R))) % N) / N))
+            Ns *= R
+    return np.array(out)
+
+
+def model_fft(x, N, E, rads, tab, toff):
+    TL = N // E
+    R0 = rads[0]
+    v = [[x[q + TL * b + r * (N // R0)] for b in range(E // R0) for r in range(R0)] for q in range(TL)]
+    Ns, off = 1, toff
+    smem_max = -1
+    for si, R in enumerate(rads):
+        for q in range(TL):
+            for b in range(E // R):
+                k = (q + TL * b) % Ns
+                for r in range(1, R):
+                    if Ns > 1:
+                        idx = off + r * Ns + k
+                        assert idx < len(tab)
+                        v[q][b * R + r] *= tab[idx]
+                v[q][b * R:(b + 1) * R] = list(np.fft.fft(np.array(v[q][b * R:(b + 1) * R])))
+        if si + 1 < len(rads):
+            Rn = rads[si + 1]
+            buf = np.full(N, np.nan, complex)
+            for q in range(TL):
+                for b in range(E // R):
+                    j = q + TL * b
+                    k = j % Ns
+                    for r in range(R):
+                        pos = (j - k) * R + k + r * Ns
+                        assert 0 <= pos < N and np.isnan(buf[pos])  # each slot written once
+                        smem_max = max(smem_max, pos + pos // 16)
+                        buf[pos] = v[q][b * R + r]
+            v = [[buf[q + TL * b + r * (N // Rn)] for b in range(E // Rn) for r in range(Rn)]
+                 for q in range(TL)]
+        off += R * Ns
+        Ns *= R
+    RL = rads[-1]
+    out = np.zeros(N, complex)
+    for q in range(TL):
+        for b in range(E // RL):
+            for r in range(RL):
+                out[q + TL * b + r * (N // RL)] = v[q][b * RL + r]
+    assert smem_max < N + N // 16 or len(rads) == 1
+    return out
+
+
+@pytest.mark.parametrize("plan", COMPILED_PLANS, ids=[str(p[0]) for p in COMPILED_PLANS])
+def test_compiled_plan_index_model(plan):
+    N, E, rads = plan
+    assert np.prod(rads) == N and all(E % R == 0 for R in rads) and 32 % (N // E) == 0
+    tab = stage_table(N, rads)
+    fwd_entries = sum(R * int(np.prod(rads[:i])) for i, R in enumerate(rads))
+    rng = np.random.default_rng(N)
+    x = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    y = model_fft(x, N, E, rads, tab, 0)
+    assert np.allclose(y, np.fft.fft(x), rtol=0, atol=1e-10 * np.abs(y).max())
+    # the reversed plan consumes the forward plan's register layout directly
+    z = model_fft(y, N, E, tuple(reversed(rads)), tab, fwd_entries)
+    assert np.allclose(z, np.fft.fft(np.fft.fft(x)), rtol=0, atol=1e-10 * np.abs(z).max())
