@@ -155,6 +155,17 @@ SES_API ses_status ses_gpu_psi_device(ses_handle h, void** dptr, size_t* bytes);
  *   [6] total batch (first to last event)   [7] number of launches
  * Unused kinds report 0.  psi advances exactly as with ses_gpu_step.  Blocks. */
 SES_API ses_status ses_gpu_profile_step(ses_handle h, int nsteps, int absorb, double* pass_ms);
+/* Tile-shape autotuner (plays the role of the reference's VkFFT plan set-up,
+ * solver/src/vk_engine.ixx:3220-3306): times every compiled tile variant of
+ * each axis pass (tile width, ring depth, warps per CTA, register budget) and
+ * the register-path kernels on the handle's scratch field -- psi is not
+ * touched -- and keeps the fastest per axis.  flags bit 0: also record the
+ * choice in the on-disk cache ($SES_TUNE_CACHE, default
+ * ~/.cache/ses_b200/autotune.txt), which later handles of the same shape read
+ * at creation.  Blocks. */
+SES_API ses_status ses_gpu_autotune(ses_handle h, int flags);
+/* Human-readable description of the handle's axis plans and chosen variants. */
+SES_API ses_status ses_gpu_plan_info(ses_handle h, char* buf, size_t len);
 /* Device bytes held by the handle. */
 SES_API ses_status ses_gpu_footprint(ses_handle h, size_t* bytes);
 

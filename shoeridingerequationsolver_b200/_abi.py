@@ -22,7 +22,7 @@ EXPORTS = [
     "ses_gpu_set_absorber_separable", "ses_gpu_step", "ses_gpu_fft3", "ses_gpu_tables",
     "ses_gpu_dt", "ses_gpu_observe", "ses_gpu_read_psi", "ses_gpu_write_psi", "ses_gpu_sync",
     "ses_gpu_set_stream", "ses_gpu_psi_device", "ses_gpu_footprint", "ses_fft3_host",
-    "ses_gpu_profile_step",
+    "ses_gpu_profile_step", "ses_gpu_autotune", "ses_gpu_plan_info",
 ]
 
 
@@ -84,6 +84,8 @@ def _load() -> C.CDLL:
         "ses_gpu_footprint": ([hp, C.POINTER(C.c_size_t)], st),
         "ses_fft3_host": ([C.POINTER(C.c_int32), C.c_int, dp, C.c_int], st),
         "ses_gpu_profile_step": ([hp, C.c_int, C.c_int, dp], st),
+        "ses_gpu_autotune": ([hp, C.c_int], st),
+        "ses_gpu_plan_info": ([hp, C.c_char_p, C.c_size_t], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -301,6 +301,16 @@ class SplitOperator3D:
         d["launches"] = int(out[7])
         return d
 
+    def autotune(self, save: bool = True) -> str:
+        """Time the compiled tile variants of each axis pass and keep the fastest."""
+        check(lib.ses_gpu_autotune(self._h, 1 if save else 0))
+        return self.plan_info()
+
+    def plan_info(self) -> str:
+        buf = C.create_string_buffer(512)
+        check(lib.ses_gpu_plan_info(self._h, buf, 512))
+        return buf.value.decode()
+
     def footprint(self) -> int:
         b = C.c_size_t()
         check(lib.ses_gpu_footprint(self._h, C.byref(b)))

@@ -1,13 +1,19 @@
 // Host side of the C ABI declared in include/ses_gpu.h: axis plans, the
 // solver handle (resident psi + FP64-built tables in HBM), the Strang step
 // program, observables and the fft / tables surfaces.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <sys/stat.h>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
 #include <string>
 #include <thread>
 #include <vector>
@@ -237,6 +243,17 @@ struct ses_solver {
 
     cudaGraphExec_t body[2] = {nullptr, nullptr};
     size_t bytes = 0;
+
+    // pipelined passes: TMA descriptors of psi / scratch along y and z, per variant
+    static constexpr int kMaxVar = 4;
+    CUtensorMap tmap[2][3][kMaxVar];
+    bool tmap_ok[2][3][kMaxVar] = {};
+    unsigned* derr = nullptr;  // device error word written by bounded waits
+    unsigned* herr = nullptr;  // pinned host copy
+    int sms = 148;
+    bool pipelined = true;
+    int xsel = 0;                  // pipelined contiguous-pass variant (-1: register path)
+    int ssel[3] = {0, 0, 0};       // pipelined strided-pass variant per axis (-1: register path)
 };
 
 namespace {
@@ -276,6 +293,8 @@ void release(ses_solver* h) {
         if (h->stwl[a]) cudaFree(h->stwl[a]);
     }
     if (h->hsums) cudaFreeHost(h->hsums);
+    if (h->herr) cudaFreeHost(h->herr);
+    if (h->derr) cudaFree(h->derr);
     if (h->ev) cudaEventDestroy(h->ev);
     if (h->cap) cudaStreamDestroy(h->cap);
     if (h->own) cudaStreamDestroy(h->own);
@@ -290,11 +309,19 @@ void set_smem_attr(K kernel) {
 // Bounded wait on everything queued so far on the handle's stream.
 ses_status wait_bounded(ses_solver* h, int timeout_ms) {
     if (timeout_ms <= 0) timeout_ms = 10000;
+    if (h->derr) SES_CU(cudaMemcpyAsync(h->herr, h->derr, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
     SES_CU(cudaEventRecord(h->ev, h->stream));
     const auto t0 = std::chrono::steady_clock::now();
     for (;;) {
         const cudaError_t q = cudaEventQuery(h->ev);
-        if (q == cudaSuccess) return SES_OK;
+        if (q == cudaSuccess) {
+            if (h->herr && *h->herr) {
+                *h->herr = 0;
+                cudaMemsetAsync(h->derr, 0, sizeof(unsigned), h->stream);
+                return fail(SES_ETIMEDOUT, "a pipelined pass gave up waiting for its tile loads");
+            }
+            return SES_OK;
+        }
         if (q != cudaErrorNotReady)
             return fail(SES_EDEVICE, std::string("device error: ") + cudaGetErrorString(q));
         const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
@@ -383,8 +410,41 @@ ses_status launch(const ses_solver* h, int axis, int mode, const PassArgs<T>& a,
     const PassPlan& pp = h->pp[axis];
     if (pp.cp) {
         const PlanEntry<T>* e = reinterpret_cast<const PlanEntry<T>*>(pp.cp);
-        PassKernel<T> k = axis == 0 ? e->xk[mode] : e->sk[mode];
-        k<<<pp.cgrid, pp.cblock, pp.csmem, s>>>(a);
+        const int n = h->n[axis];
+        const int tl = n / e->e;
+        bool done = false;
+        const int xs = h->xsel, ss = h->ssel[axis];
+        if (h->pipelined && axis == 0 && xs >= 0 && xs < (int)e->xv.size() && e->xv[xs].k[mode] &&
+            e->xv[xs].bps[mode] > 0) {
+            const auto& v = e->xv[xs];
+            PipeArgs pa{};
+            pa.ntiles = (int)((pp.nlines + v.lpc - 1) / v.lpc);
+            pa.err = h->derr;
+            const int grid = std::min(pa.ntiles, h->sms * v.bps[mode]);
+            v.k[mode]<<<grid, 32 * v.warps, v.smem[mode], s>>>(a, pa);
+            done = true;
+        } else if (h->pipelined && axis != 0 && ss >= 0 && ss < (int)e->sv.size() && e->sv[ss].k[mode] &&
+                   e->sv[ss].bps[mode] > 0) {
+            const auto& v = e->sv[ss];
+            const int buf = a.src == reinterpret_cast<const cx<T>*>(h->psi) ? 0
+                            : (a.src == reinterpret_cast<const cx<T>*>(h->scratch) ? 1 : -1);
+            if (buf >= 0 && ss < ses_solver::kMaxVar && h->tmap_ok[buf][axis][ss] && a.src == a.dst &&
+                (axis == 2 || h->n[0] % v.ls == 0)) {
+                PipeArgs pa{};
+                pa.ntiles = (int)((pp.nlines + v.ls - 1) / v.ls);
+                pa.kind = axis == 1 ? 0 : 1;
+                pa.rows_per_box = n > 256 ? 256 : n;
+                pa.nbox = n / pa.rows_per_box;
+                pa.err = h->derr;
+                const int grid = std::min(pa.ntiles, h->sms * v.bps[mode]);
+                v.k[mode]<<<grid, v.ls * tl, v.smem, s>>>(a, h->tmap[buf][axis][ss], pa);
+                done = true;
+            }
+        }
+        if (!done) {
+            PassKernel<T> k = axis == 0 ? e->xk[mode] : e->sk[mode];
+            k<<<pp.cgrid, pp.cblock, pp.csmem, s>>>(a);
+        }
     } else {
         XKernel<T> k = axis == 0 ? xkernel<T>(mode) : skernel<T>(mode);
         k<<<pp.grid, pp.g.nthreads, pp.smem, s>>>(a);
@@ -698,6 +758,169 @@ ses_status profile_batch(ses_solver* h, int S, bool mask, double* out) {
     return st;
 }
 
+// ---------------------------------------------------------------------------
+// Tile-variant selection and autotuning
+// ---------------------------------------------------------------------------
+std::string tune_cache_path() {
+    if (const char* p = std::getenv("SES_TUNE_CACHE")) return p;
+    const char* home = std::getenv("HOME");
+    return std::string(home ? home : "/tmp") + "/.cache/ses_b200/autotune.txt";
+}
+
+std::string tune_key(const ses_solver* h, int axis) {
+    std::ostringstream k;
+    const char* role = axis == 0 ? "x" : (axis == h->last_axis ? "fused" : "s");
+    k << "sm" << h->sms << ":" << (h->prec == SES_C128 ? "c128" : "c64") << ":" << role << ":"
+      << h->n[axis] << ":" << h->pp[axis].nlines;
+    return k.str();
+}
+
+std::map<std::string, int> read_tune_cache() {
+    std::map<std::string, int> m;
+    std::ifstream f(tune_cache_path());
+    std::string key;
+    int v;
+    while (f >> key >> v) m[key] = v;
+    return m;
+}
+
+void write_tune_cache(const std::map<std::string, int>& add) {
+    std::map<std::string, int> m = read_tune_cache();
+    for (const auto& kv : add) m[kv.first] = kv.second;
+    const std::string path = tune_cache_path();
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos) {
+        std::string dir = path.substr(0, slash);
+        std::string cmd;
+        for (size_t i = 1; i <= dir.size(); ++i)  // mkdir -p without a shell
+            if (i == dir.size() || dir[i] == '/') {
+                const std::string sub = dir.substr(0, i);
+                mkdir(sub.c_str(), 0755);
+            }
+    }
+    std::ofstream f(path, std::ios::trunc);
+    for (const auto& kv : m) f << kv.first << " " << kv.second << "\n";
+}
+
+template <typename T>
+int variant_count(const ses_solver* h, int axis) {
+    const PlanEntry<T>* e = reinterpret_cast<const PlanEntry<T>*>(h->pp[axis].cp);
+    if (!e) return 0;
+    return axis == 0 ? (int)e->xv.size() : (int)std::min<size_t>(e->sv.size(), ses_solver::kMaxVar);
+}
+
+// Selections at creation: cache, then environment overrides SES_XVAR / SES_SVAR.
+void apply_selection(ses_solver* h) {
+    const std::map<std::string, int> cache = read_tune_cache();
+    for (int a = 0; a < 3; ++a) {
+        auto it = cache.find(tune_key(h, a));
+        if (it == cache.end()) continue;
+        if (a == 0) h->xsel = it->second;
+        else h->ssel[a] = it->second;
+    }
+    if (const char* e = std::getenv("SES_XVAR")) h->xsel = std::atoi(e);
+    if (const char* e = std::getenv("SES_SVAR")) h->ssel[1] = h->ssel[2] = std::atoi(e);
+}
+
+// Mean ms of `reps` launches of the axis's step pass on the scratch field.
+template <typename T>
+ses_status time_axis_pass(ses_solver* h, int axis, int reps, float* ms) {
+    cudaStream_t s = h->stream;
+    auto one = [&]() -> ses_status {
+        if (axis == 0) {
+            XProg p;
+            if (h->last_axis == 0) {
+                p.mode = XM_FWD;  // 1D handles run XM_1D, which has no pipelined variant
+            } else {
+                p.mode = XM_MID;
+                p.d_mid = DG_FULL;
+                p.m_mid = h->has_mask;
+            }
+            return pass_x<T>(h, h->scratch, h->scratch, p, s);
+        }
+        return pass_s<T>(h, axis, h->scratch, h->scratch, axis == h->last_axis ? SM_FUSED : SM_FWD, 1.0, s);
+    };
+    for (int i = 0; i < 2; ++i) SES_TRY(one());
+    cudaEvent_t e0, e1;
+    SES_CU(cudaEventCreate(&e0));
+    SES_CU(cudaEventCreate(&e1));
+    cudaEventRecord(e0, s);
+    ses_status st = SES_OK;
+    for (int i = 0; i < reps && st == SES_OK; ++i) st = one();
+    cudaEventRecord(e1, s);
+    if (st == SES_OK) st = wait_bounded(h, 60000);
+    float t = 0.f;
+    if (st == SES_OK) cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / reps;
+    return st;
+}
+
+template <typename T>
+ses_status autotune_impl(ses_solver* h, int flags) {
+    std::map<std::string, int> chosen;
+    const bool saved_pipe = h->pipelined;
+    h->pipelined = true;
+    for (int axis = 0; axis < 3; ++axis) {
+        if (h->n[axis] < 2 || !h->pp[axis].cp) continue;
+        if (axis > 0 && axis != h->last_axis && axis != 1) continue;
+        const int nv = variant_count<T>(h, axis);
+        int best = -1;
+        float best_ms = 1e30f;
+        for (int c = -1; c < nv; ++c) {
+            if (axis == 0) h->xsel = c;
+            else h->ssel[axis] = c;
+            float ms = 0.f;
+            SES_TRY(time_axis_pass<T>(h, axis, 5, &ms));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+        if (axis == 0) h->xsel = best;
+        else h->ssel[axis] = best;
+        chosen[tune_key(h, axis)] = best;
+    }
+    h->pipelined = saved_pipe;
+    drop_graphs(h);
+    if (flags & 1) write_tune_cache(chosen);
+    return SES_OK;
+}
+
+template <typename T>
+std::string plan_info_t(const ses_solver* h) {
+    std::ostringstream o;
+    const char* names[3] = {"x", "y", "z"};
+    for (int a = 0; a < 3; ++a) {
+        o << names[a] << ":" << h->n[a];
+        const PlanEntry<T>* e = reinterpret_cast<const PlanEntry<T>*>(h->pp[a].cp);
+        if (h->n[a] < 2) {
+            o << " (untransformed)";
+        } else if (!e) {
+            o << " run-time plan (" << h->pp[a].g.nst << " stages)";
+        } else {
+            o << " compiled " << e->r0;
+            if (e->r1 > 1) o << "x" << e->r1;
+            if (e->r2 > 1) o << "x" << e->r2;
+            o << " E=" << e->e;
+            const int sel = a == 0 ? h->xsel : h->ssel[a];
+            const int nv = a == 0 ? (int)e->xv.size() : (int)e->sv.size();
+            if (!h->pipelined || sel < 0 || sel >= nv) {
+                o << " register-path";
+            } else if (a == 0) {
+                o << " pipelined warps=" << e->xv[sel].warps << " ring=" << e->xv[sel].nbuf << " (variant "
+                  << sel << ")";
+            } else {
+                o << " pipelined TMA lines=" << e->sv[sel].ls << " ring=" << e->sv[sel].nbuf << " (variant "
+                  << sel << ")";
+            }
+        }
+        if (a < 2) o << "; ";
+    }
+    return o.str();
+}
+
 ses_status check_handle(ses_handle h) {
     if (!h) return fail(SES_EINVAL, "null handle");
     return SES_OK;
@@ -781,6 +1004,73 @@ ses_status upload_stage_twiddles(ses_solver* h) {
         }
     }
     return SES_OK;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// TMA descriptors for the strided passes over `base` (psi or scratch), one per
+// pipelined variant (the box width is the variant's tile width L):
+// y pass: 3D {nx, ny, nz} boxes {L, rows, 1}; z pass: 2D {nx*ny, nz} boxes {L, rows};
+// elements addressed as 8-byte words (complex128 = 2 words).
+template <typename T>
+void build_tmaps_t(ses_solver* h, int buf, void* base, EncodeTiledFn enc) {
+    for (int axis = 1; axis < 3; ++axis) {
+        const PassPlan& pp = h->pp[axis];
+        if (!pp.cp || h->n[axis] < 2) continue;
+        const auto* e = reinterpret_cast<const PlanEntry<T>*>(pp.cp);
+        const int n = h->n[axis];
+        const cuuint32_t rows = (cuuint32_t)(n > 256 ? 256 : n);
+        if (n % (int)rows) continue;
+        const cuuint64_t ew = (cuuint64_t)(h->esize / 8);
+        const cuuint64_t nx = h->n[0], ny = h->n[1], nz = h->n[2];
+        for (int k = 0; k < (int)e->sv.size() && k < ses_solver::kMaxVar; ++k) {
+            const int ls = e->sv[k].ls;
+            CUresult r;
+            if (axis == 1) {
+                if (nx % (cuuint64_t)ls) continue;  // a tile must not cross z
+                const cuuint64_t dims[3] = {nx * ew, ny, nz};
+                const cuuint64_t strides[2] = {nx * h->esize, nx * ny * h->esize};
+                const cuuint32_t box[3] = {(cuuint32_t)(ls * ew), rows, 1};
+                const cuuint32_t es[3] = {1, 1, 1};
+                r = enc(&h->tmap[buf][axis][k], CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            } else {
+                const cuuint64_t dims[2] = {nx * ny * ew, nz};
+                const cuuint64_t strides[1] = {nx * ny * h->esize};
+                const cuuint32_t box[2] = {(cuuint32_t)(ls * ew), rows};
+                const cuuint32_t es[2] = {1, 1};
+                r = enc(&h->tmap[buf][axis][k], CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            }
+            h->tmap_ok[buf][axis][k] = (r == CUDA_SUCCESS);
+        }
+    }
+}
+
+void build_tmaps(ses_solver* h, int buf, void* base) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return;
+    if (h->prec == SES_C128) build_tmaps_t<double>(h, buf, base, enc);
+    else build_tmaps_t<float>(h, buf, base, enc);
 }
 
 ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt, double mass,
@@ -867,6 +1157,19 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
     }
     if (cudaGetLastError() != cudaSuccess) return bail(fail(SES_EDEVICE, "axis table build failed"));
     if ((st = upload_stage_twiddles(h)) != SES_OK) return bail(st);
+    if ((st = dalloc(h, (void**)&h->derr, sizeof(unsigned))) != SES_OK) return bail(st);
+    if (cudaMallocHost((void**)&h->herr, sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(fail(SES_ENOMEM, "pinned host allocation failed"));
+    }
+    *h->herr = 0;
+    if (cudaMemsetAsync(h->derr, 0, sizeof(unsigned), h->stream) != cudaSuccess)
+        return bail(fail(SES_EDEVICE, "memset failed"));
+    cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->dev);
+    if (const char* env = std::getenv("SES_PIPELINED")) h->pipelined = std::atoi(env) != 0;
+    build_tmaps(h, 0, h->psi);
+    build_tmaps(h, 1, h->scratch);
+    apply_selection(h);
     if (with_tables) {
         if ((st = dalloc(h, (void**)&h->V, N * sizeof(double))) != SES_OK) return bail(st);
         if ((st = dalloc(h, &h->vtab, N * h->esize)) != SES_OK) return bail(st);
@@ -1138,6 +1441,20 @@ ses_status ses_gpu_profile_step(ses_handle h, int nsteps, int absorb, double* pa
     const bool mask = absorb != 0 && h->has_mask;
     return h->prec == SES_C128 ? profile_batch<double>(h, nsteps, mask, pass_ms)
                                : profile_batch<float>(h, nsteps, mask, pass_ms);
+}
+
+ses_status ses_gpu_autotune(ses_handle h, int flags) {
+    SES_TRY(check_handle(h));
+    SES_TRY(wait_bounded(h, 0));
+    return h->prec == SES_C128 ? autotune_impl<double>(h, flags) : autotune_impl<float>(h, flags);
+}
+
+ses_status ses_gpu_plan_info(ses_handle h, char* buf, size_t len) {
+    SES_TRY(check_handle(h));
+    if (!buf || len == 0) return fail(SES_EINVAL, "null buffer");
+    const std::string info = h->prec == SES_C128 ? plan_info_t<double>(h) : plan_info_t<float>(h);
+    std::snprintf(buf, len, "%s", info.c_str());
+    return SES_OK;
 }
 
 ses_status ses_gpu_footprint(ses_handle h, size_t* bytes) {

@@ -85,6 +85,30 @@ __device__ __forceinline__ cx<T> apply_diag(cx<T> v, int kind, int use_mask, lon
     return narrow<T>(p);
 }
 
+// Same as apply_diag with the potential-table entry and mask value supplied
+// by the caller (pipelined passes stage the table in shared memory).
+template <typename T>
+__device__ __forceinline__ cx<T> apply_diag_tv(cx<T> v, int kind, cx<T> tab, int use_mask, double m) {
+    cx<double> p = widen(v);
+    if (kind != DG_NONE) {
+        if constexpr (sizeof(T) == 8) {
+            const cx<double> h = widen(tab);
+            p = p * (kind == DG_FULL ? h * h : h);
+        } else {
+            cx<double> d = widen(tab);
+            if (kind == DG_FULL)  // (1 + d)^2 - 1 = 2d + d^2
+                d = mk<double>(2.0 * d.x + (d.x * d.x - d.y * d.y), 2.0 * d.y + 2.0 * d.x * d.y);
+            p = p + p * d;
+        }
+    }
+    if (use_mask) p = mk<double>(p.x * m, p.y * m);
+    return narrow<T>(p);
+}
+
+__device__ __forceinline__ double mask_at(const Tables& tb, long long f, int i, int j, int k) {
+    return tb.maskfull ? tb.maskfull[f] : tb.mask1[0][i] * tb.mask1[1][j] * tb.mask1[2][k];
+}
+
 // (1+a)(1+b) - 1 for the separable kinetic deltas
 __device__ __forceinline__ cx<double> dmul1(cx<double> a, cx<double> b) { return a + b + a * b; }
 

@@ -1,0 +1,303 @@
+// Pipelined compiled-plan passes: persistent CTAs walk the tiles of a pass
+// while a ring of NBUF shared-memory tile buffers is filled asynchronously --
+// strided axes by TMA tensor loads (boxes of L lines x up to 256 rows), the
+// contiguous axis by 1D bulk copies of whole lines (psi and, where the pass
+// applies the potential, the matching rows of the potential table).  The FFT
+// of tile i overlaps the loads of tiles i+1 .. i+NBUF-1.  Exchanges between
+// Stockham stages reuse the tile buffer in place; results go to HBM with
+// coalesced stores.
+#pragma once
+
+#include "ses_pass2.cuh"
+#include "ses_tma.cuh"
+
+namespace sesk {
+
+struct PipeArgs {
+    int ntiles;         // tiles of the pass
+    int kind;           // strided: 0 -> 3D map {nx, ny, nz} (y pass), 1 -> 2D map {nx*ny, nz} (z pass)
+    int rows_per_box;   // <= 256
+    int nbox;           // boxes per tile along the transformed axis
+    unsigned* err;      // device error word (bit 0: a bounded wait expired)
+};
+
+// XOR-swizzled position inside a dense line: bijective on [0, N) for N % 16 == 0,
+// spreads both exchange patterns of the compiled plans over the banks.
+__device__ __forceinline__ int swz(int pos) { return pos ^ ((pos >> 4) & 15); }
+
+template <typename T>
+struct XchLine {
+    cx<T>* p;
+    __device__ __forceinline__ void put(int pos, cx<T> v) { p[swz(pos)] = v; }
+    __device__ __forceinline__ cx<T> get(int pos) const { return p[swz(pos)]; }
+    __device__ __forceinline__ void sync() { __syncwarp(); }
+};
+
+// Abort after an expired wait: record it, drain this CTA's outstanding copies
+// (bounded), return.  Called by all threads of the CTA together.
+__device__ __forceinline__ void pipe_abort(const PipeArgs& pa, const uint64_t* bars, int nbuf, int i,
+                                           int nmine) {
+    if (threadIdx.x == 0) atomicOr(pa.err, 1u);
+    for (int j = i; j < nmine && j < i + nbuf; ++j)
+        (void)mbar_wait(smem_u32(&bars[j % nbuf]), (uint32_t)((j / nbuf) & 1));
+}
+
+// ---------------------------------------------------------------------------
+// Strided axis (y or z).  CTA = L lines x N/E threads; tile = N rows x L lines.
+// ---------------------------------------------------------------------------
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, int NBUF, int MINB>
+__global__ void __launch_bounds__(L*(N / E), MINB)
+    spass3_kernel(const PassArgs<T> a, const __grid_constant__ CUtensorMap tmap, const PipeArgs pa) {
+    constexpr int TL = N / E;
+    constexpr int EW = (int)sizeof(cx<T>) / 8;  // 8-byte words per element
+    constexpr uint32_t TILE_BYTES = (uint32_t)(N * L * sizeof(cx<T>));
+    using S = PlanShape<R0, R1, R2>;
+    constexpr int RL = S::last;
+    extern __shared__ __align__(1024) unsigned char smraw3[];
+    cx<T>* tiles = reinterpret_cast<cx<T>*>(smraw3);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smraw3 + (size_t)NBUF * TILE_BYTES);
+    const int l = threadIdx.x % L, q = threadIdx.x / L;
+    const int nmine = blockIdx.x < (unsigned)pa.ntiles ? (pa.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < NBUF; ++b) mbar_init(smem_u32(&bars[b]), 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int i) {  // thread 0: load this CTA's i-th tile into buffer i % NBUF
+        const int buf = i % NBUF;
+        const long long s0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * L;
+        const uint32_t bar = smem_u32(&bars[buf]);
+        const uint32_t dst = smem_u32(tiles + (size_t)buf * N * L);
+        mbar_expect_tx(bar, TILE_BYTES);
+        for (int bx = 0; bx < pa.nbox; ++bx) {
+            const uint32_t d = dst + (uint32_t)(bx * pa.rows_per_box * L * (int)sizeof(cx<T>));
+            if (pa.kind == 0)
+                tma_load_3d(d, &tmap, (int)(s0 % a.nx) * EW, bx * pa.rows_per_box, (int)(s0 / a.nx), bar);
+            else
+                tma_load_2d(d, &tmap, (int)s0 * EW, bx * pa.rows_per_box, bar);
+        }
+    };
+    if (threadIdx.x == 0)
+        for (int i = 0; i < NBUF && i < nmine; ++i) issue(i);
+
+    const bool ypass = a.axis == 1;
+    for (int i = 0; i < nmine; ++i) {
+        const int buf = i % NBUF;
+        const bool ok = mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i / NBUF) & 1));
+        if (__syncthreads_or(!ok)) {
+            pipe_abort(pa, bars, NBUF, i, nmine);
+            return;
+        }
+        cx<T>* tile = tiles + (size_t)buf * N * L;
+        const long long s = (long long)((int)blockIdx.x + i * (int)gridDim.x) * L + l;
+        const bool valid = s < a.nlines;
+        const long long sc_ = valid ? s : 0;
+        const long long w = (long long)fdiv((uint32_t)sc_, a.fnu);
+        const long long u = sc_ - w * a.nu;
+        const long long base = u + w * a.sw;
+        XchCta<T, L> x{tile, l};
+        cx<T> v[E];
+#pragma unroll
+        for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const cx<T> e = tile[(q + TL * b + r * (N / R0)) * L + l];
+                v[b * R0 + r] = MODE == SM_INV ? cconj(e) : e;
+            }
+        __syncthreads();  // all stage-0 reads before the tile is reused for exchanges
+        rfft_plan<T, N, E, R0, R1, R2, false>(v, q, a.stw, a.stwl, x);
+
+        int c1, c2;
+        if (ypass) {
+            c1 = (int)u;
+            c2 = (int)w;
+        } else {
+            c2 = (int)fdiv((uint32_t)u, a.fnx);
+            c1 = (int)(u - (long long)c2 * a.nx);
+        }
+        if constexpr (MODE == SM_FWD || MODE == SM_INV) {
+            const T scl = (T)a.out_scale;
+            if (valid) {
+#pragma unroll
+                for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const int pos = q + TL * b + r * (N / RL);
+                        cx<T> e = v[b * RL + r];
+                        if constexpr (MODE == SM_INV) e = scale(cconj(e), scl);
+                        a.dst[base + pos * a.se] = e;
+                    }
+            }
+        } else if constexpr (MODE == SM_FUSED) {
+            const cx<double> dother = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
+            const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
+#pragma unroll
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const int pos = q + TL * b + r * (N / RL);
+                    v[b * RL + r] = kinetic_conj(v[b * RL + r], dmul1(dother, kda[pos]), a.tb.kscale);
+                }
+            rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+            if (valid) {
+#pragma unroll
+                for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                    for (int r = 0; r < R0; ++r) {
+                        const int pos = q + TL * b + r * (N / R0);
+                        a.dst[base + pos * a.se] = cconj(v[b * R0 + r]);
+                    }
+            }
+        }
+        // release the buffer: generic accesses ordered before the next TMA write
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0 && i + NBUF < nmine) issue(i + NBUF);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Contiguous axis (x).  NW warps per CTA, a warp owns 32/(N/E) lines; a tile
+// is the CTA's consecutive lines, copied whole (plus the potential-table rows
+// when the mode applies the potential).
+// ---------------------------------------------------------------------------
+template <int MODE>
+struct XUsesTable {
+    static constexpr bool value = MODE == XM_START || MODE == XM_MID || MODE == XM_END || MODE == XM_1D;
+};
+
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int NW, int NBUF, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T> a, const PipeArgs pa) {
+    constexpr int TL = N / E;
+    constexpr int LPW = 32 / TL;
+    constexpr int LPC = NW * LPW;
+    constexpr bool kTab = XUsesTable<MODE>::value;
+    constexpr uint32_t PSI_BYTES = (uint32_t)(LPC * N * sizeof(cx<T>));
+    constexpr uint32_t BUF_BYTES = kTab ? 2 * PSI_BYTES : PSI_BYTES;
+    using S = PlanShape<R0, R1, R2>;
+    constexpr int RF = R0, RL = S::last;
+    extern __shared__ __align__(1024) unsigned char smraw3[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smraw3 + (size_t)NBUF * BUF_BYTES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lw = lane / TL, q = lane % TL;
+    const int nmine = blockIdx.x < (unsigned)pa.ntiles ? (pa.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const cx<T>* vtab = reinterpret_cast<const cx<T>*>(a.tb.vtab);
+
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < NBUF; ++b) mbar_init(smem_u32(&bars[b]), 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int i) {
+        const int buf = i % NBUF;
+        const long long m0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * LPC;
+        const long long rem = a.nlines - m0;
+        const int nval = rem < LPC ? (int)rem : LPC;
+        const uint32_t bytes = (uint32_t)(nval * N * (int)sizeof(cx<T>));
+        const uint32_t bar = smem_u32(&bars[buf]);
+        const uint32_t dst = smem_u32(smraw3 + (size_t)buf * BUF_BYTES);
+        mbar_expect_tx(bar, kTab ? 2 * bytes : bytes);
+        bulk_g2s(dst, a.src + m0 * N, bytes, bar);
+        if constexpr (kTab) bulk_g2s(dst + PSI_BYTES, vtab + m0 * N, bytes, bar);
+    };
+    if (threadIdx.x == 0)
+        for (int i = 0; i < NBUF && i < nmine; ++i) issue(i);
+
+    for (int i = 0; i < nmine; ++i) {
+        const int buf = i % NBUF;
+        const bool ok = mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i / NBUF) & 1));
+        if (__syncthreads_or(!ok)) {
+            pipe_abort(pa, bars, NBUF, i, nmine);
+            return;
+        }
+        cx<T>* ptile = reinterpret_cast<cx<T>*>(smraw3 + (size_t)buf * BUF_BYTES);
+        const cx<T>* ttile = reinterpret_cast<const cx<T>*>(smraw3 + (size_t)buf * BUF_BYTES + PSI_BYTES);
+        const int lc = warp * LPW + lw;  // line within the tile
+        const long long m = (long long)((int)blockIdx.x + i * (int)gridDim.x) * LPC + lc;
+        const bool valid = m < a.nlines;
+        const long long mc = valid ? m : 0;
+        const int kz = (int)fdiv((uint32_t)mc, a.fny);
+        const int jy = (int)(mc - (long long)kz * a.ny);
+        cx<T>* line = ptile + (size_t)lc * N;
+        const cx<T>* tline = ttile + (size_t)lc * N;
+        XchLine<T> x{line};
+        cx<T>* dst = a.dst + mc * N;
+        cx<T> v[E];
+        constexpr bool kConjIn = MODE == XM_MID || MODE == XM_END;
+#pragma unroll
+        for (int b = 0; b < E / RF; ++b)
+#pragma unroll
+            for (int r = 0; r < RF; ++r) {
+                const int pos = q + TL * b + r * (N / RF);
+                cx<T> e = line[pos];
+                if constexpr (MODE == XM_START || MODE == XM_1D) {
+                    if (a.d_load != DG_NONE || a.m_load)
+                        e = apply_diag_tv(e, a.d_load, tline[pos], a.m_load,
+                                          a.m_load ? mask_at(a.tb, mc * N + pos, pos, jy, kz) : 1.0);
+                }
+                v[b * RF + r] = kConjIn ? cconj(e) : e;
+            }
+        __syncwarp();  // the line is reused for exchanges: all stage-0 reads first
+        rfft_plan<T, N, E, R0, R1, R2, false>(v, q, a.stw, a.stwl, x);
+
+        if constexpr (MODE == XM_FWD || MODE == XM_START || MODE == XM_END) {
+            if (valid) {
+#pragma unroll
+                for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const int pos = q + TL * b + r * (N / RL);
+                        cx<T> e = v[b * RL + r];
+                        if constexpr (MODE == XM_END) {
+                            e = cconj(e);
+                            if (a.d_store != DG_NONE || a.m_store)
+                                e = apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
+                                                  a.m_store ? mask_at(a.tb, mc * N + pos, pos, jy, kz) : 1.0);
+                        }
+                        dst[pos] = e;
+                    }
+            }
+        } else if constexpr (MODE == XM_MID || MODE == XM_1D) {
+            const cx<double> dyz = dmul1(a.tb.kd[1][jy], a.tb.kd[2][kz]);
+#pragma unroll
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const int pos = q + TL * b + r * (N / RL);
+                    cx<T> e = v[b * RL + r];
+                    if constexpr (MODE == XM_MID) {
+                        e = cconj(e);
+                        if (a.d_mid != DG_NONE || a.m_mid)
+                            e = apply_diag_tv(e, a.d_mid, tline[pos], a.m_mid,
+                                              a.m_mid ? mask_at(a.tb, mc * N + pos, pos, jy, kz) : 1.0);
+                    } else {
+                        e = kinetic_conj(e, dmul1(dyz, a.tb.kd[0][pos]), a.tb.kscale);
+                    }
+                    v[b * RL + r] = e;
+                }
+            rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+            if (valid) {
+#pragma unroll
+                for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                    for (int r = 0; r < R0; ++r) {
+                        const int pos = q + TL * b + r * (N / R0);
+                        cx<T> e = v[b * R0 + r];
+                        if constexpr (MODE == XM_1D) {
+                            e = cconj(e);
+                            if (a.d_store != DG_NONE || a.m_store)
+                                e = apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
+                                                  a.m_store ? mask_at(a.tb, mc * N + pos, pos, jy, kz) : 1.0);
+                        }
+                        dst[pos] = e;
+                    }
+            }
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0 && i + NBUF < nmine) issue(i + NBUF);
+    }
+}
+
+}  // namespace sesk

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "ses_pass2.cuh"
+#include "ses_pass3.cuh"
 
 namespace sesk {
 
@@ -19,6 +20,23 @@ struct PlanEntry {
     int xw = 4;             // warps per contiguous-pass CTA
     PassKernel<T> xk[7];    // by XMode
     PassKernel<T> sk[4];    // by SModeK
+    // pipelined variants; the solver picks one per axis (default 0, or autotuned)
+    using XPipe = void (*)(const PassArgs<T>, const PipeArgs);
+    using SPipe = void (*)(const PassArgs<T>, const CUtensorMap, const PipeArgs);
+    struct XVar {
+        XPipe k[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+        int warps = 0, lpc = 0, nbuf = 0;
+        size_t smem[7] = {0, 0, 0, 0, 0, 0, 0};
+        int bps[7] = {0, 0, 0, 0, 0, 0, 0};  // resident CTAs per SM
+    };
+    struct SVar {
+        SPipe k[4] = {nullptr, nullptr, nullptr, nullptr};
+        int ls = 0, nbuf = 0;
+        size_t smem = 0;
+        int bps[4] = {0, 0, 0, 0};
+    };
+    std::vector<XVar> xv;
+    std::vector<SVar> sv;
 };
 
 template <typename K>
@@ -50,6 +68,51 @@ PlanEntry<T> make_plan_entry() {
     const int smem = N * LS * (int)sizeof(cx<T>);
     for (auto k : p.sk) allow_smem(k, smem);
     return p;
+}
+
+// Pipelined variants: contiguous pass with NW warps per CTA, strided pass with
+// LS lines per CTA; NBUF-deep tile rings; MINB = CTAs per SM the register
+// allocation is sized for.
+template <typename T, int N, int E, int R0, int R1, int R2, int NW, int NBUF, int MINB>
+void add_x_variant(PlanEntry<T>& p) {
+    constexpr int TL = N / E;
+    constexpr int LPC = NW * (32 / TL);
+    typename PlanEntry<T>::XVar v;
+    v.warps = NW;
+    v.lpc = LPC;
+    v.nbuf = NBUF;
+    v.k[XM_FWD] = xpass3_kernel<T, XM_FWD, N, E, R0, R1, R2, NW, NBUF, MINB>;
+    v.k[XM_START] = xpass3_kernel<T, XM_START, N, E, R0, R1, R2, NW, NBUF, MINB>;
+    v.k[XM_MID] = xpass3_kernel<T, XM_MID, N, E, R0, R1, R2, NW, NBUF, MINB>;
+    v.k[XM_END] = xpass3_kernel<T, XM_END, N, E, R0, R1, R2, NW, NBUF, MINB>;
+    const size_t psi = (size_t)LPC * N * sizeof(cx<T>);
+    for (int m : {XM_FWD, XM_START, XM_MID, XM_END}) {
+        v.smem[m] = NBUF * (m != XM_FWD ? 2 * psi : psi) + NBUF * sizeof(uint64_t);
+        allow_smem(v.k[m], (int)v.smem[m]);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bps[m], v.k[m], NW * 32, v.smem[m],
+                                                              cudaOccupancyDefault);
+    }
+    cudaGetLastError();
+    p.xv.push_back(v);
+}
+
+template <typename T, int N, int E, int R0, int R1, int R2, int LS, int NBUF, int MINB>
+void add_s_variant(PlanEntry<T>& p) {
+    constexpr int TL = N / E;
+    typename PlanEntry<T>::SVar v;
+    v.ls = LS;
+    v.nbuf = NBUF;
+    v.k[SM_FWD] = spass3_kernel<T, SM_FWD, N, E, R0, R1, R2, LS, NBUF, MINB>;
+    v.k[SM_INV] = spass3_kernel<T, SM_INV, N, E, R0, R1, R2, LS, NBUF, MINB>;
+    v.k[SM_FUSED] = spass3_kernel<T, SM_FUSED, N, E, R0, R1, R2, LS, NBUF, MINB>;
+    v.smem = NBUF * (size_t)N * LS * sizeof(cx<T>) + NBUF * sizeof(uint64_t);
+    for (int m : {SM_FWD, SM_INV, SM_FUSED}) {
+        allow_smem(v.k[m], (int)v.smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bps[m], v.k[m], LS * TL, v.smem,
+                                                              cudaOccupancyDefault);
+    }
+    cudaGetLastError();
+    p.sv.push_back(v);
 }
 
 // defined in ses_plans_*.cu

@@ -8,7 +8,11 @@ void register_plans_small(std::vector<PlanEntry<float>>& f, std::vector<PlanEntr
     f.push_back(make_plan_entry<float, 32, 8, 8, 4, 1, 32>());
     d.push_back(make_plan_entry<double, 32, 8, 8, 4, 1, 16>());
     f.push_back(make_plan_entry<float, 64, 8, 8, 8, 1, 32>());
+    add_x_variant<float, 64, 8, 8, 8, 1, 4, 2, 2>(f.back());
+    add_s_variant<float, 64, 8, 8, 8, 1, 32, 2, 2>(f.back());
     d.push_back(make_plan_entry<double, 64, 8, 8, 8, 1, 16>());
+    add_x_variant<double, 64, 8, 8, 8, 1, 4, 2, 2>(d.back());
+    add_s_variant<double, 64, 8, 8, 8, 1, 16, 2, 2>(d.back());
     f.push_back(make_plan_entry<float, 128, 16, 16, 8, 1, 32>());
     d.push_back(make_plan_entry<double, 128, 16, 16, 8, 1, 16>());
 }
