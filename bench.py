@@ -54,6 +54,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-requests", type=int, default=5)
     ap.add_argument("--segment", type=int, default=100, help="steps per end-to-end request")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the cached / SES_XVAR, SES_SVAR tile variants instead of tuning")
     ap.add_argument("--quick", action="store_true",
                     help="timed region and per-pass profile only (for profiler launch lists)")
     ap.add_argument("--accuracy-steps", type=int, default=-1,
@@ -272,7 +274,8 @@ def measure_precision(ses, w, prec, K, W, stream, dist, world, clocks_gpu):
     if absorb:
         op.set_absorber_separable(*w.mask)
     op.set_stream(stream.cuda_stream)
-    plan = op.autotune(save=False)  # pick tile variants on the scratch field (untimed)
+    # pick tile variants on the scratch field (untimed)
+    plan = op.plan_info() if NO_AUTOTUNE else op.autotune(save=False)
     op.upload_state(w.psi0)
     warm = max(W, 9)  # >= 9 so the captured step graph exists before timing
     op.advance(warm, absorb=absorb)
@@ -440,8 +443,13 @@ def run_ours(args):
     return 0
 
 
+NO_AUTOTUNE = False
+
+
 def main(argv=None):
+    global NO_AUTOTUNE
     args = parse_args(argv)
+    NO_AUTOTUNE = args.no_autotune
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -228,6 +228,8 @@ struct ses_solver {
     double* kv[3] = {nullptr, nullptr, nullptr};
     cx<double>* kd[3] = {nullptr, nullptr, nullptr};
     double* mask1[3] = {nullptr, nullptr, nullptr};
+    float* mask1f[3] = {nullptr, nullptr, nullptr};
+    cx<float>* kdf[3] = {nullptr, nullptr, nullptr};
     double* maskfull = nullptr;
     bool has_mask = false;
 
@@ -289,6 +291,8 @@ void release(ses_solver* h) {
         if (h->kv[a]) cudaFree(h->kv[a]);
         if (h->kd[a]) cudaFree(h->kd[a]);
         if (h->mask1[a]) cudaFree(h->mask1[a]);
+        if (h->mask1f[a]) cudaFree(h->mask1f[a]);
+        if (h->kdf[a]) cudaFree(h->kdf[a]);
         if (h->stw[a]) cudaFree(h->stw[a]);
         if (h->stwl[a]) cudaFree(h->stwl[a]);
     }
@@ -371,6 +375,8 @@ PassArgs<T> make_args(const ses_solver* h, int axis, const void* src, void* dst)
         tb.mask1[q] = h->mask1[q];
         tb.kd[q] = h->kd[q];
         tb.kv[q] = h->kv[q];
+        tb.mask1f[q] = h->mask1f[q];
+        tb.kdf[q] = h->kdf[q];
     }
     tb.maskfull = h->maskfull;
     tb.inv_mass = 1.0 / h->mass;
@@ -1154,6 +1160,8 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
         build_axis_tables<<<gb, 256, 0, h->stream>>>(h->box[2 * a], h->box[2 * a + 1], n,
                                                      with_tables ? dt : 0.0,
                                                      with_tables ? mass : 1.0, h->kv[a], h->kd[a]);
+        if ((st = dalloc(h, (void**)&h->kdf[a], (size_t)n * sizeof(cx<float>))) != SES_OK) return bail(st);
+        convert_kernel<double, float><<<gb, 256, 0, h->stream>>>(h->kd[a], h->kdf[a], n);
     }
     if (cudaGetLastError() != cudaSuccess) return bail(fail(SES_EDEVICE, "axis table build failed"));
     if ((st = upload_stage_twiddles(h)) != SES_OK) return bail(st);
@@ -1244,7 +1252,10 @@ ses_status ses_gpu_set_absorber_separable(ses_handle h, const double* mx, const 
     }
     for (int a = 0; a < 3; ++a) {
         if (!h->mask1[a]) SES_TRY(dalloc(h, (void**)&h->mask1[a], (size_t)h->n[a] * sizeof(double)));
+        if (!h->mask1f[a]) SES_TRY(dalloc(h, (void**)&h->mask1f[a], (size_t)h->n[a] * sizeof(float)));
         SES_CU(cudaMemcpy(h->mask1[a], m[a], (size_t)h->n[a] * sizeof(double), cudaMemcpyHostToDevice));
+        std::vector<float> mf(m[a], m[a] + h->n[a]);
+        SES_CU(cudaMemcpy(h->mask1f[a], mf.data(), (size_t)h->n[a] * sizeof(float), cudaMemcpyHostToDevice));
     }
     h->has_mask = true;
     return SES_OK;
@@ -1282,7 +1293,9 @@ ses_status ses_gpu_set_absorber(ses_handle h, const double* mask) {
     if (separable) return ses_gpu_set_absorber_separable(h, mx.data(), my.data(), mz.data());
     for (int a = 0; a < 3; ++a) {
         if (h->mask1[a]) cudaFree(h->mask1[a]);
+        if (h->mask1f[a]) cudaFree(h->mask1f[a]);
         h->mask1[a] = nullptr;
+        h->mask1f[a] = nullptr;
     }
     if (!h->maskfull) SES_TRY(dalloc(h, (void**)&h->maskfull, h->N * sizeof(double)));
     SES_CU(cudaMemcpy(h->maskfull, mask, h->N * sizeof(double), cudaMemcpyHostToDevice));

@@ -34,9 +34,26 @@ struct Tables {
     const double* maskfull;    // non-separable absorber (nullable)
     const cx<double>* kd[3];   // per axis: cis(-k^2 dt/(2m)) - 1
     const double* kv[3];       // per axis: wavenumbers (fftfreq layout)
+    // complex64 path: the same FP64-built per-axis tables rounded to FP32
+    const float* mask1f[3];
+    const cx<float>* kdf[3];
     double inv_mass;
     double kscale;             // 1/N, folded into the kinetic multiply
 };
+
+// complex64 phase multiplies in FP32 on the delta form: psi + psi*d, d = factor - 1.
+// (1 + d)^2 - 1 = 2d + d^2 for the full potential kick between steps.
+__device__ __forceinline__ cx<float> delta_full(cx<float> d) {
+    return mk<float>(fmaf(d.x, d.x, fmaf(-d.y, d.y, 2.0f * d.x)), fmaf(2.0f * d.x, d.y, 2.0f * d.y));
+}
+__device__ __forceinline__ cx<float> add_mul(cx<float> p, cx<float> d) {  // p + p*d
+    return mk<float>(fmaf(p.x, d.x, fmaf(-p.y, d.y, p.x)), fmaf(p.x, d.y, fmaf(p.y, d.x, p.y)));
+}
+// (1+a)(1+b) - 1 for the separable kinetic deltas
+__device__ __forceinline__ cx<double> dmul1(cx<double> a, cx<double> b) { return a + b + a * b; }
+__device__ __forceinline__ cx<float> dmul1f(cx<float> a, cx<float> b) {  // (1+a)(1+b) - 1
+    return mk<float>(fmaf(a.x, b.x, fmaf(-a.y, b.y, a.x + b.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, a.y + b.y)));
+}
 
 template <typename T>
 struct PassArgs {
@@ -61,10 +78,27 @@ struct PassArgs {
     double* partials;
 };
 
+// Absorber value at flat index f, coordinates (i, j, k): m = mx[i] * (my[j] * mz[k])
+// (complex64 path: FP32 product of mx[i] and the FP32-rounded line factor).
+template <typename T>
+__device__ __forceinline__ double maskval(const Tables& tb, long long f, int i, int j, int k) {
+    if (tb.maskfull) return tb.maskfull[f];
+    const double lyz = tb.mask1[1][j] * tb.mask1[2][k];
+    if constexpr (sizeof(T) == 4) return (double)(tb.mask1f[0][i] * (float)lyz);
+    else return tb.mask1[0][i] * lyz;
+}
+
+template <typename T>
+__device__ __forceinline__ cx<T> apply_diag_tv(cx<T> v, int kind, cx<T> tab, int use_mask, double m);
+
 // psi * (potential phase) * (mask) at flat index f, coordinates (i, j, k).
 template <typename T>
 __device__ __forceinline__ cx<T> apply_diag(cx<T> v, int kind, int use_mask, long long f, int i, int j,
                                             int k, const Tables& tb) {
+    if constexpr (sizeof(T) == 4) {
+        const cx<T> tab = kind != DG_NONE ? reinterpret_cast<const cx<T>*>(tb.vtab)[f] : v;
+        return apply_diag_tv(v, kind, tab, use_mask, use_mask ? maskval<T>(tb, f, i, j, k) : 1.0);
+    }
     cx<double> p = widen(v);
     if (kind != DG_NONE) {
         if constexpr (sizeof(T) == 8) {
@@ -78,17 +112,26 @@ __device__ __forceinline__ cx<T> apply_diag(cx<T> v, int kind, int use_mask, lon
         }
     }
     if (use_mask) {
-        const double m = tb.maskfull ? tb.maskfull[f]
-                                     : tb.mask1[0][i] * tb.mask1[1][j] * tb.mask1[2][k];
+        const double m = maskval<T>(tb, f, i, j, k);
         p = mk<double>(p.x * m, p.y * m);
     }
     return narrow<T>(p);
 }
 
 // Same as apply_diag with the potential-table entry and mask value supplied
-// by the caller (pipelined passes stage the table in shared memory).
+// by the caller (pipelined passes stage the table in shared memory).  The
+// complex64 path multiplies in FP32 on the delta form.
 template <typename T>
 __device__ __forceinline__ cx<T> apply_diag_tv(cx<T> v, int kind, cx<T> tab, int use_mask, double m) {
+    if constexpr (sizeof(T) == 4) {
+        cx<float> p = v;
+        if (kind != DG_NONE) p = add_mul(p, kind == DG_FULL ? delta_full(tab) : tab);
+        if (use_mask) {
+            const float mf = (float)m;
+            p = mk<float>(p.x * mf, p.y * mf);
+        }
+        return p;
+    }
     cx<double> p = widen(v);
     if (kind != DG_NONE) {
         if constexpr (sizeof(T) == 8) {
@@ -109,8 +152,19 @@ __device__ __forceinline__ double mask_at(const Tables& tb, long long f, int i, 
     return tb.maskfull ? tb.maskfull[f] : tb.mask1[0][i] * tb.mask1[1][j] * tb.mask1[2][k];
 }
 
-// (1+a)(1+b) - 1 for the separable kinetic deltas
-__device__ __forceinline__ cx<double> dmul1(cx<double> a, cx<double> b) { return a + b + a * b; }
+// psi_k * K / N then conj (inverse FFT start); complex64: FP32 on the delta form.
+__device__ __forceinline__ cx<float> kinetic_conj_f(cx<float> v, cx<float> d, float kscale) {
+    const cx<float> p = add_mul(v, d);
+    return mk<float>(p.x * kscale, -p.y * kscale);
+}
+
+template <typename T>
+__device__ __forceinline__ cx<T> kinetic_apply(cx<T> v, cx<double> dother, const cx<double>* kda64,
+                                               const cx<float>* kda32, int pos, double kscale) {
+    if constexpr (sizeof(T) == 4) return kinetic_conj_f(v, dmul1f(narrow<float>(dother), kda32[pos]), (float)kscale);
+    else return kinetic_conj(v, dmul1(dother, kda64[pos]), kscale);
+}
+
 
 // psi_k * K(k) / N followed by the conjugation that starts the inverse FFT.
 template <typename T>
@@ -119,6 +173,13 @@ __device__ __forceinline__ cx<T> kinetic_conj(cx<T> v, cx<double> d, double ksca
     p = p + p * d;
     return narrow<T>(mk<double>(p.x * kscale, -p.y * kscale));
 }
+
+// Kinetic multiply of element `pos` of an axis whose other two axes give the
+// FP64 delta `dother`: complex128 -> FP64; complex64 -> FP32 delta form with
+// the FP32-rounded tables (kda64 / kda32 are the axis's FP64 / FP32 deltas).
+template <typename T>
+__device__ __forceinline__ cx<T> kinetic_apply(cx<T> v, cx<double> dother, const cx<double>* kda64,
+                                               const cx<float>* kda32, int pos, double kscale);
 
 template <int NR>
 __device__ __forceinline__ void block_reduce_store(double (&acc)[NR], double* out) {
@@ -245,8 +306,8 @@ __global__ void __launch_bounds__(512, 1) xpass_kernel(const PassArgs<T> a) {
             const long long m = m0l < a.nlines ? m0l : 0;
             const int k = (int)fdiv((uint32_t)m, a.fny);
             const int j = (int)(m - (long long)k * a.ny);
-            const cx<double> d = dmul1(dmul1(a.tb.kd[1][j], a.tb.kd[2][k]), a.tb.kd[0][e]);
-            sm[l * g.ls + e] = kinetic_conj(v, d, a.tb.kscale);
+            sm[l * g.ls + e] = kinetic_apply(v, dmul1(a.tb.kd[1][j], a.tb.kd[2][k]), a.tb.kd[0], a.tb.kdf[0],
+                                             e, a.tb.kscale);
         };
         fft_tile<T, kEPTDev, false, false>(g, sm, a.tw, lds, stk);
         auto stc = [&](int l, int e, cx<T> v) { sm[l * g.ls + e] = cconj(v); };
@@ -362,8 +423,8 @@ __global__ void __launch_bounds__(512, 1) spass_kernel(const PassArgs<T> a) {
         fft_tile<T, kEPTDev, true, true>(g, sm, a.tw, ldc, stc);
     } else if constexpr (MODE == SM_FUSED) {
         auto stk = [&](int l, int e, cx<T> v) {
-            const cx<double> d = dmul1(dother[l], kda[e]);
-            sm[l * g.ls + e * g.es] = kinetic_conj(v, d, a.tb.kscale);
+            sm[l * g.ls + e * g.es] = kinetic_apply(v, dother[l], kda, ypass ? a.tb.kdf[1] : a.tb.kdf[2], e,
+                                                    a.tb.kscale);
         };
         fft_tile<T, kEPTDev, true, false>(g, sm, a.tw, ldg, stk);
         auto lds = [&](int l, int e) -> cx<T> { return sm[l * g.ls + e * g.es]; };

@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4) xpass2_kernel(con
                     if (a.d_mid != DG_NONE || a.m_mid)
                         e = apply_diag(e, a.d_mid, a.m_mid, mc * N + pos, pos, jy, kz, a.tb);
                 } else {
-                    e = kinetic_conj(e, dmul1(dyz, a.tb.kd[0][pos]), a.tb.kscale);
+                    e = kinetic_apply(e, dyz, a.tb.kd[0], a.tb.kdf[0], pos, a.tb.kscale);
                 }
                 v[b * RL + r] = e;
             }
@@ -336,12 +336,13 @@ __global__ void __launch_bounds__(L*(N / E), 1) spass2_kernel(const PassArgs<T> 
     if constexpr (MODE == SM_FUSED) {
         const cx<double> dother = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
         const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
+        const cx<float>* kdaf = ypass ? a.tb.kdf[1] : a.tb.kdf[2];
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
 #pragma unroll
             for (int r = 0; r < RL; ++r) {
                 const int pos = q + TL * b + r * (N / RL);
-                v[b * RL + r] = kinetic_conj(v[b * RL + r], dmul1(dother, kda[pos]), a.tb.kscale);
+                v[b * RL + r] = kinetic_apply(v[b * RL + r], dother, kda, kdaf, pos, a.tb.kscale);
             }
         rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
         if (valid) {

@@ -132,12 +132,13 @@ __global__ void __launch_bounds__(L*(N / E), MINB)
         } else if constexpr (MODE == SM_FUSED) {
             const cx<double> dother = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
             const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
+            const cx<float>* kdaf = ypass ? a.tb.kdf[1] : a.tb.kdf[2];
 #pragma unroll
             for (int b = 0; b < E / RL; ++b)
 #pragma unroll
                 for (int r = 0; r < RL; ++r) {
                     const int pos = q + TL * b + r * (N / RL);
-                    v[b * RL + r] = kinetic_conj(v[b * RL + r], dmul1(dother, kda[pos]), a.tb.kscale);
+                    v[b * RL + r] = kinetic_apply(v[b * RL + r], dother, kda, kdaf, pos, a.tb.kscale);
                 }
             rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
             if (valid) {
@@ -219,6 +220,15 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
         const long long mc = valid ? m : 0;
         const int kz = (int)fdiv((uint32_t)mc, a.fny);
         const int jy = (int)(mc - (long long)kz * a.ny);
+        // separable absorber: per-line factor my[j] * mz[k] (the mask is m = mx[i] * (my[j] * mz[k]))
+        const bool sep = a.tb.maskfull == nullptr && a.tb.mask1[0] != nullptr;
+        const double myz = sep ? a.tb.mask1[1][jy] * a.tb.mask1[2][kz] : 1.0;
+        const float myzf = (float)myz;
+        auto mval = [&](int pos) -> double {  // == maskval<T>(a.tb, mc * N + pos, pos, jy, kz)
+            if (!sep) return a.tb.maskfull ? a.tb.maskfull[mc * N + pos] : 1.0;
+            if constexpr (sizeof(T) == 4) return (double)(a.tb.mask1f[0][pos] * myzf);
+            else return a.tb.mask1[0][pos] * myz;
+        };
         cx<T>* line = ptile + (size_t)lc * N;
         const cx<T>* tline = ttile + (size_t)lc * N;
         XchLine<T> x{line};
@@ -234,7 +244,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
                 if constexpr (MODE == XM_START || MODE == XM_1D) {
                     if (a.d_load != DG_NONE || a.m_load)
                         e = apply_diag_tv(e, a.d_load, tline[pos], a.m_load,
-                                          a.m_load ? mask_at(a.tb, mc * N + pos, pos, jy, kz) : 1.0);
+                                          a.m_load ? mval(pos) : 1.0);
                 }
                 v[b * RF + r] = kConjIn ? cconj(e) : e;
             }
@@ -253,7 +263,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
                             e = cconj(e);
                             if (a.d_store != DG_NONE || a.m_store)
                                 e = apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
-                                                  a.m_store ? mask_at(a.tb, mc * N + pos, pos, jy, kz) : 1.0);
+                                                  a.m_store ? mval(pos) : 1.0);
                         }
                         dst[pos] = e;
                     }
@@ -270,7 +280,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
                         e = cconj(e);
                         if (a.d_mid != DG_NONE || a.m_mid)
                             e = apply_diag_tv(e, a.d_mid, tline[pos], a.m_mid,
-                                              a.m_mid ? mask_at(a.tb, mc * N + pos, pos, jy, kz) : 1.0);
+                                              a.m_mid ? mval(pos) : 1.0);
                     } else {
                         e = kinetic_conj(e, dmul1(dyz, a.tb.kd[0][pos]), a.tb.kscale);
                     }
@@ -288,7 +298,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
                             e = cconj(e);
                             if (a.d_store != DG_NONE || a.m_store)
                                 e = apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
-                                                  a.m_store ? mask_at(a.tb, mc * N + pos, pos, jy, kz) : 1.0);
+                                                  a.m_store ? mval(pos) : 1.0);
                         }
                         dst[pos] = e;
                     }
