@@ -169,6 +169,30 @@ SES_API ses_status ses_gpu_plan_info(ses_handle h, char* buf, size_t len);
 /* Device bytes held by the handle. */
 SES_API ses_status ses_gpu_footprint(ses_handle h, size_t* bytes);
 
+/* ---- allocation-free entry point ----
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- a host framework whose caching allocator already owns the GPU's
+ * memory, where a cudaMalloc from this library could fail, or a loop that
+ * must not pay cudaMalloc/cudaFree synchronisation: the real-space
+ * observables of a caller-owned device field, with no handle and no device
+ * allocation of any kind.
+ *   psi_dev  nx*ny*nz complex128 (SES_C128) or complex64 (SES_C64) values, x-fastest
+ *   V_dev    nx*ny*nz doubles, or NULL (then out[1] = 0)
+ *   out_dev  9 doubles in device memory: norm, <V>, probability in [xlo, xhi),
+ *            mean position x y z, sigma x y z (same definitions as ses_gpu_observe)
+ *   cuda_stream  the stream to run on (NULL: the default stream); the call
+ *            returns once the work is queued
+ * Scratch is a fixed 2.25 MiB array in the library's device image, held by
+ * every GPU that loads the library until the process exits, so grids are
+ * limited to 2^27 points (512^3): larger grids return SES_EINVAL.  All calls
+ * on a device share that array: calls that overlap on the GPU (different
+ * streams, or different host threads) race and must be serialised by the
+ * caller.  The first call on each device resolves the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. */
+SES_API ses_status ses_observe_real_noalloc(const ses_grid_desc* grid, ses_precision prec,
+                                            const void* psi_dev, const double* V_dev, double xlo,
+                                            double xhi, double* out_dev, void* cuda_stream);
+
 /* ---- fft surface on host arrays (core/src/fft.ixx:75-188) ----
  * fft(std::vector<cd>&) / ifft(...) and fft(Field3D&) / ifft(Field3D&):
  * n[3] = (nx, ny, nz), data = interleaved complex128, transformed in place

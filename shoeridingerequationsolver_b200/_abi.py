@@ -22,7 +22,7 @@ EXPORTS = [
     "ses_gpu_set_absorber_separable", "ses_gpu_step", "ses_gpu_fft3", "ses_gpu_tables",
     "ses_gpu_dt", "ses_gpu_observe", "ses_gpu_read_psi", "ses_gpu_write_psi", "ses_gpu_sync",
     "ses_gpu_set_stream", "ses_gpu_psi_device", "ses_gpu_footprint", "ses_fft3_host",
-    "ses_gpu_profile_step", "ses_gpu_autotune", "ses_gpu_plan_info",
+    "ses_gpu_profile_step", "ses_gpu_autotune", "ses_gpu_plan_info", "ses_observe_real_noalloc",
 ]
 
 
@@ -86,6 +86,8 @@ def _load() -> C.CDLL:
         "ses_gpu_profile_step": ([hp, C.c_int, C.c_int, dp], st),
         "ses_gpu_autotune": ([hp, C.c_int], st),
         "ses_gpu_plan_info": ([hp, C.c_char_p, C.c_size_t], st),
+        "ses_observe_real_noalloc": ([C.POINTER(GridDesc), C.c_int, vp, vp, C.c_double, C.c_double, vp,
+                                      vp], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

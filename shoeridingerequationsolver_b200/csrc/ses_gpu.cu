@@ -205,6 +205,10 @@ bool plan_pass(int n, int esize, bool strided, long long nlines, PassPlan& pp, s
 
 }  // namespace
 
+namespace sesk {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace sesk
+
 struct ses_solver {
     int dev = 0;
     ses_precision prec = SES_C128;

@@ -1,0 +1,67 @@
+"""Allocation-free real-space observables (ses_observe_real_noalloc).
+
+The entry point serves callers that cannot allocate device memory -- a host
+framework whose caching allocator already owns the GPU (a library cudaMalloc
+could fail), or a loop that must not pay cudaMalloc synchronisation.  It takes
+the field, the potential and the 9-double output in the caller's device memory
+and keeps its per-CTA partial sums in a fixed array inside the library.  These
+tests call it through the C ABI twice in a row and compare with the handle
+based ses_gpu_observe, which reduces the same field with its own buffers.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+TOL = 1e-12  # both reduce the same values in FP64; only the summation order differs
+
+
+def _grid(ses, box, n):
+    return ses.Grid3D(*(ses.Grid1D(box[2 * a], box[2 * a + 1], n[a]) for a in range(3)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_noalloc_matches_observe_on_two_calls(ses, oracle, prec):
+    import torch
+    from shoeridingerequationsolver_b200 import _abi
+    from shoeridingerequationsolver_b200.core import PRECISIONS
+
+    box, n = (-10.0, 10.0, -8.0, 8.0, -6.0, 6.0), (64, 48, 40)
+    V = oracle.harmonic3d(box, n, 0.9, (0.5, -0.25, 0.0))
+    psi = oracle.gaussian3d(box, n, (1.5, -0.5, 0.25), (1.2, 1.0, 0.9), (0.6, 0.0, -0.4))
+    op = ses.SplitOperator3D(_grid(ses, box, n), V, 0.01, precision=prec)
+    op.upload_state(psi)
+    op.advance(3)
+    ref = op.observe(0.5, 7.0)
+    op.sync()
+    psi_ptr, _ = op.psi_device()
+
+    V_dev = torch.from_numpy(V).to("cuda")        # caller-owned device buffers
+    out = torch.full((9,), float("nan"), dtype=torch.float64, device="cuda")
+    desc = _abi.grid_desc(_grid(ses, box, n))
+    expect = np.array([ref["norm"], ref["energy_v"], ref["p_range"], *ref["mean_pos"], *ref["sigma_pos"]])
+    for call in range(2):                          # the shared scratch carries over between calls
+        out.fill_(float("nan"))
+        st = _abi.lib.ses_observe_real_noalloc(C.byref(desc), PRECISIONS[prec], C.c_void_p(psi_ptr),
+                                              C.c_void_p(V_dev.data_ptr()), 0.5, 7.0,
+                                              C.c_void_p(out.data_ptr()), None)
+        assert st == _abi.SES_OK, _abi.last_error()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.all(np.isfinite(got)), (call, got)
+        assert np.allclose(got, expect, rtol=TOL, atol=TOL), (call, got, expect)
+    op.close()
+
+
+def test_noalloc_rejects_grids_beyond_its_scratch():
+    import shoeridingerequationsolver_b200 as ses
+    from shoeridingerequationsolver_b200 import _abi
+
+    # 1024 x 1024 x 129 points needs more partial-sum rows than the fixed array holds
+    desc = _abi.grid_desc(_grid(ses, (0.0, 1.0) * 3, (1024, 1024, 129)))
+    st = _abi.lib.ses_observe_real_noalloc(C.byref(desc), _abi.SES_C64, C.c_void_p(16), None, 0.0, 1.0,
+                                          C.c_void_p(16), None)
+    assert st == _abi.SES_EINVAL
+    assert "2^27" in _abi.last_error()
