@@ -193,6 +193,54 @@ SES_API ses_status ses_observe_real_noalloc(const ses_grid_desc* grid, ses_preci
                                             const void* psi_dev, const double* V_dev, double xlo,
                                             double xhi, double* out_dev, void* cuda_stream);
 
+/* ---- batches: many independent propagations per launch ----
+ * The reference advances one field per Engine (solver/src/vk_engine.ixx:
+ * 597-698) and batches sweeps on the CPU by parallel_for over instances
+ * (core/src/parallel.ixx:195-238); a batch replaces that loop.  Handles join a
+ * batch; members with the same grid shape and precision form a class, and each
+ * axis pass of a step is ONE launch per class whose CTAs walk instance x
+ * line tiles.  Classes run concurrently on their own streams; interior steps
+ * are CUDA graphs.  Every member keeps its own field, potential table, axis
+ * tables, dt, mass and absorber, and computes exactly what ses_gpu_step would
+ * with the same step batching.  Shapes without batched kernels step member by
+ * member.  A member's stream is the batch's stream while it belongs to it;
+ * calls on a member (observe, read_psi, ...) stay valid and are ordered after
+ * the batch's queued steps.  Destroying a member removes it first.  A batch
+ * is single-threaded like a handle. */
+typedef struct ses_batch_s* ses_batch;
+SES_API ses_status ses_batch_create(ses_batch* out);
+SES_API ses_status ses_batch_destroy(ses_batch b);
+/* SES_EBUSY if h already belongs to a batch; waits for h's queued work. */
+SES_API ses_status ses_batch_add(ses_batch b, ses_handle h);
+SES_API ses_status ses_batch_remove(ses_batch b, ses_handle h);
+/* Every member advances nsteps merged Strang steps (absorb: members that have an
+ * absorber apply it after every step).  Returns once the work is queued; the
+ * first call after a membership change waits for queued work and uploads the
+ * per-member pass arguments. */
+SES_API ses_status ses_batch_step(ses_batch b, int nsteps, int absorb);
+/* ses_gpu_observe of every member, in the order they were added (count must be
+ * the member count), with one wait for the whole batch. */
+SES_API ses_status ses_batch_observe(ses_batch b, double xlo, double xhi, ses_observables* out, int count);
+SES_API ses_status ses_batch_sync(ses_batch b, int timeout_ms);
+SES_API ses_status ses_batch_set_stream(ses_batch b, void* cuda_stream);
+SES_API ses_status ses_batch_members(ses_batch b, int* members, int* classes);
+/* Per class (in order of first appearance), 5 values: mean milliseconds per
+ * launch of the x pass between steps, the strided passes 1..3 of the step, and
+ * their sum (one interior step of the whole class), timed with events around
+ * nsteps interior steps run class after class on the batch stream.  Members
+ * advance by a complete Strang batch of nsteps + 1 steps (nsteps + 2 for 1D).
+ * Blocks. */
+SES_API ses_status ses_batch_profile(ses_batch b, int nsteps, int absorb, double* ms, int count);
+/* Tile-shape autotuner for every class: times the register-path and each
+ * pipelined variant of the x pass and of each strided pass on the members'
+ * scratch fields (psi is not touched) and keeps the fastest for the batch.
+ * flags bit 0: also record the choice in the on-disk cache (as
+ * ses_gpu_autotune), which later batches with a class of the same shape read.
+ * Blocks. */
+SES_API ses_status ses_batch_autotune(ses_batch b, int flags);
+/* One line per class: shape, precision, members and the kernel of each pass. */
+SES_API ses_status ses_batch_info(ses_batch b, char* buf, size_t len);
+
 /* ---- fft surface on host arrays (core/src/fft.ixx:75-188) ----
  * fft(std::vector<cd>&) / ifft(...) and fft(Field3D&) / ifft(Field3D&):
  * n[3] = (nx, ny, nz), data = interleaved complex128, transformed in place

@@ -23,6 +23,9 @@ EXPORTS = [
     "ses_gpu_dt", "ses_gpu_observe", "ses_gpu_read_psi", "ses_gpu_write_psi", "ses_gpu_sync",
     "ses_gpu_set_stream", "ses_gpu_psi_device", "ses_gpu_footprint", "ses_fft3_host",
     "ses_gpu_profile_step", "ses_gpu_autotune", "ses_gpu_plan_info", "ses_observe_real_noalloc",
+    "ses_batch_create", "ses_batch_destroy", "ses_batch_add", "ses_batch_remove", "ses_batch_step",
+    "ses_batch_observe", "ses_batch_sync", "ses_batch_set_stream", "ses_batch_members",
+    "ses_batch_profile", "ses_batch_autotune", "ses_batch_info",
 ]
 
 
@@ -88,6 +91,18 @@ def _load() -> C.CDLL:
         "ses_gpu_plan_info": ([hp, C.c_char_p, C.c_size_t], st),
         "ses_observe_real_noalloc": ([C.POINTER(GridDesc), C.c_int, vp, vp, C.c_double, C.c_double, vp,
                                       vp], st),
+        "ses_batch_create": ([C.POINTER(vp)], st),
+        "ses_batch_destroy": ([vp], st),
+        "ses_batch_add": ([vp, hp], st),
+        "ses_batch_remove": ([vp, hp], st),
+        "ses_batch_step": ([vp, C.c_int, C.c_int], st),
+        "ses_batch_observe": ([vp, C.c_double, C.c_double, C.POINTER(Observables), C.c_int], st),
+        "ses_batch_sync": ([vp, C.c_int], st),
+        "ses_batch_set_stream": ([vp, vp], st),
+        "ses_batch_members": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], st),
+        "ses_batch_profile": ([vp, C.c_int, C.c_int, dp, C.c_int], st),
+        "ses_batch_autotune": ([vp, C.c_int], st),
+        "ses_batch_info": ([vp, C.c_char_p, C.c_size_t], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

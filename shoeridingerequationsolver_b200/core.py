@@ -318,8 +318,12 @@ class SplitOperator3D:
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            check(lib.ses_gpu_destroy(self._h))
+            check(lib.ses_gpu_destroy(self._h))   # leaves its batch first
             self._h = None
+            b = getattr(self, "_batch", None)
+            if b is not None and self in b._members:
+                b._members.remove(self)
+            self._batch = None
 
     def __del__(self):
         try:
@@ -357,3 +361,90 @@ class SplitOperator1D:
 
     def close(self) -> None:
         self._op.close()
+
+
+class Batch:
+    """Many independent propagations advanced together (the reference batches
+    sweeps on the CPU with parallel_for over instances, core/src/parallel.ixx:
+    195-238).  Members are SplitOperator3D handles; members of one shape and
+    precision share one launch per axis pass, classes of different shapes run
+    concurrently."""
+
+    def __init__(self, members=()):
+        self._b = C.c_void_p()
+        check(lib.ses_batch_create(C.byref(self._b)))
+        self._members: list[SplitOperator3D] = []
+        for m in members:
+            self.add(m)
+
+    def add(self, op: SplitOperator3D) -> None:
+        check(lib.ses_batch_add(self._b, op.handle))
+        self._members.append(op)
+        op._batch = self
+
+    def remove(self, op: SplitOperator3D) -> None:
+        check(lib.ses_batch_remove(self._b, op.handle))
+        self._members.remove(op)
+        op._batch = None
+
+    @property
+    def members(self) -> list:
+        return list(self._members)
+
+    def step(self, nsteps: int, absorb: bool = False) -> None:
+        check(lib.ses_batch_step(self._b, int(nsteps), 1 if absorb else 0))
+
+    def observe(self, xlo: float = -math.inf, xhi: float = math.inf) -> list[dict]:
+        n = len(self._members)
+        out = (_abi.Observables * max(n, 1))()
+        check(lib.ses_batch_observe(self._b, float(xlo), float(xhi), out, n))
+        return [out[i].as_dict() for i in range(n)]
+
+    def sync(self, timeout_ms: int = 0) -> None:
+        check(lib.ses_batch_sync(self._b, int(timeout_ms)))
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(lib.ses_batch_set_stream(self._b, C.c_void_p(stream_ptr or 0)))
+
+    def counts(self) -> tuple[int, int]:
+        m, c = C.c_int(0), C.c_int(0)
+        check(lib.ses_batch_members(self._b, C.byref(m), C.byref(c)))
+        return m.value, c.value
+
+    def profile(self, nsteps: int, absorb: bool = False) -> list[dict]:
+        """Per class: mean ms per launch of each pass of an interior step."""
+        _, ncls = self.counts()
+        out = (C.c_double * (5 * max(ncls, 1)))()
+        check(lib.ses_batch_profile(self._b, int(nsteps), 1 if absorb else 0, out, 5 * ncls))
+        return [{"x_mid": out[5 * i], "mid": [out[5 * i + 1], out[5 * i + 2], out[5 * i + 3]],
+                 "step": out[5 * i + 4]} for i in range(ncls)]
+
+    def autotune(self, save: bool = True) -> str:
+        """Pick the fastest kernel variant of every class pass (timed on scratch fields)."""
+        check(lib.ses_batch_autotune(self._b, 1 if save else 0))
+        return self.info()
+
+    def info(self) -> str:
+        buf = C.create_string_buffer(4096)
+        check(lib.ses_batch_info(self._b, buf, 4096))
+        return buf.value.decode()
+
+    def close(self) -> None:
+        if getattr(self, "_b", None):
+            check(lib.ses_batch_destroy(self._b))
+            self._b = None
+            for op in self._members:
+                op._batch = None
+            self._members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

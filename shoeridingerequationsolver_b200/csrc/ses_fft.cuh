@@ -220,13 +220,51 @@ __device__ __forceinline__ void dft5(cx<T>* v) {
     v[3] = mk<T>(p2.x - q2.y, p2.y + q2.x);
 }
 
+// 6 = 2 x 3 and 10 = 2 x 5 by the prime-factor (Good-Thomas) mapping, which
+// needs no twiddles between the factors: input n = (R n1 + 2 n2) mod 2R,
+// output k = (R k1 + (R+1) k2) mod 2R for R = 3, 5 (CRT: R^{-1} = 1 mod 2,
+// 2^{-1} mod 3 = 2, 2^{-1} mod 5 = 3).
+template <typename T>
+__device__ __forceinline__ void dft6(cx<T>* v) {
+    cx<T> a[3] = {v[0], v[2], v[4]};
+    cx<T> b[3] = {v[3], v[5], v[1]};
+    dft3(a);
+    dft3(b);
+    v[0] = a[0] + b[0];
+    v[3] = a[0] - b[0];
+    v[4] = a[1] + b[1];
+    v[1] = a[1] - b[1];
+    v[2] = a[2] + b[2];
+    v[5] = a[2] - b[2];
+}
+
+template <typename T>
+__device__ __forceinline__ void dft10(cx<T>* v) {
+    cx<T> a[5] = {v[0], v[2], v[4], v[6], v[8]};
+    cx<T> b[5] = {v[5], v[7], v[9], v[1], v[3]};
+    dft5(a);
+    dft5(b);
+    v[0] = a[0] + b[0];
+    v[5] = a[0] - b[0];
+    v[6] = a[1] + b[1];
+    v[1] = a[1] - b[1];
+    v[2] = a[2] + b[2];
+    v[7] = a[2] - b[2];
+    v[8] = a[3] + b[3];
+    v[3] = a[3] - b[3];
+    v[4] = a[4] + b[4];
+    v[9] = a[4] - b[4];
+}
+
 template <typename T, int R>
 __device__ __forceinline__ void dft(cx<T>* v) {
     if constexpr (R == 2) dft2(v);
     else if constexpr (R == 3) dft3(v);
     else if constexpr (R == 4) dft4(v);
     else if constexpr (R == 5) dft5(v);
+    else if constexpr (R == 6) dft6(v);
     else if constexpr (R == 8) dft8(v);
+    else if constexpr (R == 10) dft10(v);
     else if constexpr (R == 16) dft16(v);
 }
 

@@ -260,6 +260,7 @@ struct ses_solver {
     bool pipelined = true;
     int xsel = 0;                  // pipelined contiguous-pass variant (-1: register path)
     int ssel[3] = {0, 0, 0};       // pipelined strided-pass variant per axis (-1: register path)
+    ses_batch_s* batch = nullptr;  // batch this handle belongs to (its stream is the batch's)
 };
 
 namespace {
@@ -1202,6 +1203,549 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
     return SES_OK;
 }
 
+// Observables from the sums enqueue_observe copied to the host (after a wait).
+void finish_observe(const ses_solver* h, ses_observables* out) {
+    const double* r = h->hsums;
+    const double* k = h->hsums + kRedR;
+    const double dv = ((h->box[1] - h->box[0]) / h->n[0]) * ((h->box[3] - h->box[2]) / h->n[1]) *
+                      ((h->box[5] - h->box[4]) / h->n[2]);
+    auto ratio = [](double num, double den) { return den > 0.0 ? num / den : 0.0; };
+    out->norm = r[0] * dv;
+    out->energy_v = ratio(r[1], r[0]);
+    out->energy_t = ratio(k[1], k[0]);
+    out->energy = out->energy_v + out->energy_t;
+    out->p_range = r[2] * dv;
+    for (int a = 0; a < 3; ++a) {
+        out->mean_pos[a] = ratio(r[3 + a], r[0]);
+        const double var = ratio(r[6 + a], r[0]) - out->mean_pos[a] * out->mean_pos[a];
+        out->sigma_pos[a] = std::sqrt(std::max(0.0, var));
+        out->mean_mom[a] = ratio(k[2 + a], k[0]);
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Batches: many handles advanced together.  Members with the same shape and
+// precision form a class; each pass of a step is ONE launch per class
+// (xbatch_kernel / sbatch_kernel walking instance x line tiles, grid sized to
+// the resident CTAs).  Every class runs its whole step sequence on its own
+// stream, forked from and joined back to the batch stream, so classes of
+// different sizes overlap on the GPU; interior steps are CUDA graphs per class.
+// ---------------------------------------------------------------------------
+enum BatchProg {
+    BP_XSTART,  // [Vh, fwd x]
+    BP_XMID,    // [inv x, V (M), fwd x]
+    BP_XEND,    // [inv x, Vh (M)]
+    BP_1DFIRST, // 1D [Vh, fwd, K/N, inv]
+    BP_1DONE,   // 1D [Vh, fwd, K/N, inv, Vh (M)]
+    BP_1DMID,   // 1D [V (M), fwd, K/N, inv]
+    BP_1DLAST,  // 1D [V (M), fwd, K/N, inv, Vh (M)]
+    BP_NX,
+    BP_MID0 = BP_NX,  // strided passes of the step, in order
+    BP_COUNT = BP_NX + 3
+};
+
+XProg batch_xprog(int prog, bool mask) {
+    XProg p;
+    switch (prog) {
+        case BP_XSTART: p.mode = XM_START; p.d_load = DG_HALF; break;
+        case BP_XMID: p.mode = XM_MID; p.d_mid = DG_FULL; p.m_mid = mask; break;
+        case BP_XEND: p.mode = XM_END; p.d_store = DG_HALF; p.m_store = mask; break;
+        case BP_1DFIRST: p.mode = XM_1D; p.d_load = DG_HALF; break;
+        case BP_1DONE:
+            p.mode = XM_1D; p.d_load = DG_HALF; p.d_store = DG_HALF; p.m_store = mask;
+            break;
+        case BP_1DMID: p.mode = XM_1D; p.d_load = DG_FULL; p.m_load = mask; break;
+        default:
+            p.mode = XM_1D; p.d_load = DG_FULL; p.m_load = mask; p.d_store = DG_HALF; p.m_store = mask;
+            break;
+    }
+    return p;
+}
+
+struct BatchClass {
+    ses_precision prec = SES_C64;
+    int n[3] = {1, 1, 1};
+    std::vector<ses_solver*> mem;
+    bool batched = false;  // every pass of the step has a batched kernel
+    int nmid = 0;
+    int mid_axis[3] = {0, 0, 0}, mid_mode[3] = {0, 0, 0};
+    size_t esz = 0;        // sizeof(PassArgs<T>)
+    void* dargs = nullptr; // [prog][mask][member] PassArgs<T>
+    size_t dcap = 0;
+    // pipelined (TMA-fed) batched variants: -1 = register-path batched kernels
+    int xvar = -1;
+    int svar[3] = {-1, -1, -1};
+    CUtensorMap* dmaps = nullptr;  // [strided pass q][member] tensor maps of the members' psi
+    size_t mcap = 0;
+    cudaStream_t cs = nullptr, cap = nullptr;
+    cudaEvent_t done = nullptr;
+    cudaGraphExec_t body[2] = {nullptr, nullptr};
+    bool dirty = true;
+};
+
+}  // namespace
+
+struct ses_batch_s {
+    int dev = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    cudaEvent_t fork = nullptr, ev = nullptr;
+    unsigned* derr = nullptr;  // device error word of the pipelined batched passes
+    unsigned* herr = nullptr;  // pinned host copy
+    std::vector<ses_solver*> members;  // in add order
+    std::vector<BatchClass*> classes;
+    std::map<std::string, int> sel;    // autotuned variant per class pass (batch_tune_key)
+    int sms = 148;
+};
+
+namespace {
+
+void drop_class(BatchClass* c) {
+    for (auto& g : c->body) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    if (c->dargs) cudaFree(c->dargs);
+    if (c->dmaps) cudaFree(c->dmaps);
+    if (c->done) cudaEventDestroy(c->done);
+    if (c->cap) cudaStreamDestroy(c->cap);
+    if (c->cs) cudaStreamDestroy(c->cs);
+    delete c;
+}
+
+ses_status batch_wait(ses_batch_s* b, int timeout_ms) {
+    if (timeout_ms <= 0) timeout_ms = 10000;
+    SES_CU(cudaMemcpyAsync(b->herr, b->derr, sizeof(unsigned), cudaMemcpyDeviceToHost, b->stream));
+    SES_CU(cudaEventRecord(b->ev, b->stream));
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(b->ev);
+        if (q == cudaSuccess) {
+            if (*b->herr) {
+                *b->herr = 0;
+                cudaMemsetAsync(b->derr, 0, sizeof(unsigned), b->stream);
+                return fail(SES_ETIMEDOUT, "a pipelined batched pass gave up waiting for its tile loads");
+            }
+            return SES_OK;
+        }
+        if (q != cudaErrorNotReady)
+            return fail(SES_EDEVICE, std::string("device error: ") + cudaGetErrorString(q));
+        const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                            std::chrono::steady_clock::now() - t0)
+                            .count();
+        if (ms > timeout_ms) return fail(SES_ETIMEDOUT, "wait exceeded " + std::to_string(timeout_ms) + " ms");
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+template <typename T>
+bool class_has_batch_kernels(const BatchClass& c) {
+    const ses_solver* h = c.mem[0];
+    for (int a = 0; a < 3; ++a) {
+        if (h->n[a] < 2 && a > 0) continue;
+        if (h->n[a] < 2) return false;  // a 1-point x axis has no compiled plan
+        const auto* e = reinterpret_cast<const PlanEntry<T>*>(h->pp[a].cp);
+        if (!e) return false;
+    }
+    return true;
+}
+
+// Cache key of a class pass: prog 0 = x pass between steps, 1 + q = strided pass q.
+std::string batch_tune_key(const ses_batch_s* b, const BatchClass& c, int prog) {
+    std::ostringstream k;
+    k << "sm" << b->sms << ":" << (c.prec == SES_C128 ? "c128" : "c64") << ":batch-"
+      << (prog == 0 ? std::string("x") : "s" + std::to_string(prog - 1)) << ":" << c.n[0] << "x" << c.n[1]
+      << "x" << c.n[2];
+    return k.str();
+}
+
+template <typename T>
+bool xvar_ok(const BatchClass& c, int k) {
+    const auto* ex = reinterpret_cast<const PlanEntry<T>*>(c.mem[0]->pp[0].cp);
+    if (k < 0 || k >= (int)ex->xv.size()) return false;
+    const auto& v = ex->xv[k];
+    for (int m : {XM_START, XM_MID, XM_END})
+        if (!v.kb[m] || v.bbps[m] <= 0) return false;
+    return true;
+}
+
+template <typename T>
+bool svar_ok(const BatchClass& c, int q, int k, int buf) {
+    const ses_solver* h0 = c.mem[0];
+    const int a = c.mid_axis[q];
+    const auto* es = reinterpret_cast<const PlanEntry<T>*>(h0->pp[a].cp);
+    if (k < 0 || k >= (int)es->sv.size() || k >= ses_solver::kMaxVar) return false;
+    const auto& v = es->sv[k];
+    if (!v.kb[c.mid_mode[q]] || v.bbps[c.mid_mode[q]] <= 0) return false;
+    if (a == 1 && h0->n[0] % v.ls) return false;
+    for (const ses_solver* h : c.mem)
+        if (!h->tmap_ok[buf][a][k]) return false;
+    return true;
+}
+
+// Variant per class pass: the batch's autotuned choice, else the on-disk cache,
+// else the first member's selection; -1 = register-path batched kernel.
+template <typename T>
+void class_select(const ses_batch_s* b, BatchClass& c) {
+    const ses_solver* h0 = c.mem[0];
+    c.xvar = -1;
+    for (int q = 0; q < 3; ++q) c.svar[q] = -1;
+    if (!h0->pipelined || h0->last_axis == 0) return;
+    const std::map<std::string, int> cache = read_tune_cache();
+    auto pick = [&](int prog, int fallback) {
+        const std::string key = batch_tune_key(b, c, prog);
+        auto it = b->sel.find(key);
+        if (it != b->sel.end()) return it->second;
+        auto jt = cache.find(key);
+        if (jt != cache.end()) return jt->second;
+        return fallback;
+    };
+    const int xs = pick(0, h0->xsel);
+    if (xvar_ok<T>(c, xs)) c.xvar = xs;
+    for (int q = 0; q < c.nmid; ++q) {
+        const int ss = pick(1 + q, h0->ssel[c.mid_axis[q]]);
+        if (svar_ok<T>(c, q, ss, 0)) c.svar[q] = ss;
+    }
+}
+
+// Tensor maps [q][member] of the members' psi (buf 0) or scratch (buf 1) for
+// the class's selected strided variants, into a device table grown as needed.
+ses_status class_maps(const BatchClass& c, int buf, CUtensorMap*& dmaps, size_t& cap) {
+    const size_t nm = c.mem.size();
+    bool any = false;
+    for (int q = 0; q < c.nmid; ++q) any = any || c.svar[q] >= 0;
+    if (!any) return SES_OK;
+    std::vector<CUtensorMap> maps((size_t)3 * nm);
+    for (int q = 0; q < c.nmid; ++q)
+        if (c.svar[q] >= 0)
+            for (size_t i = 0; i < nm; ++i) maps[(size_t)q * nm + i] = c.mem[i]->tmap[buf][c.mid_axis[q]][c.svar[q]];
+    const size_t mb = maps.size() * sizeof(CUtensorMap);
+    if (mb > cap) {
+        if (dmaps) cudaFree(dmaps);
+        dmaps = nullptr;
+        cap = 0;
+        if (cudaMalloc(&dmaps, mb) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SES_ENOMEM, "batch tensor map table allocation failed");
+        }
+        cap = mb;
+    }
+    SES_CU(cudaMemcpy(dmaps, maps.data(), mb, cudaMemcpyHostToDevice));
+    return SES_OK;
+}
+
+template <typename T>
+ses_status class_upload(const ses_batch_s* b, BatchClass& c) {
+    const size_t nm = c.mem.size();
+    const ses_solver* h0 = c.mem[0];
+    c.nmid = 0;
+    if (h0->last_axis == 2) {
+        if (h0->n[1] > 1) { c.mid_axis[c.nmid] = 1; c.mid_mode[c.nmid++] = SM_FWD; }
+        c.mid_axis[c.nmid] = 2; c.mid_mode[c.nmid++] = SM_FUSED;
+        if (h0->n[1] > 1) { c.mid_axis[c.nmid] = 1; c.mid_mode[c.nmid++] = SM_INV; }
+    } else if (h0->last_axis == 1) {
+        c.mid_axis[0] = 1; c.mid_mode[0] = SM_FUSED; c.nmid = 1;
+    }
+    c.batched = class_has_batch_kernels<T>(c);
+    if (!c.batched) return SES_OK;
+    c.esz = sizeof(PassArgs<T>);
+    std::vector<PassArgs<T>> host((size_t)BP_COUNT * 2 * nm);
+    for (int prog = 0; prog < BP_COUNT; ++prog)
+        for (int mask = 0; mask < 2; ++mask)
+            for (size_t i = 0; i < nm; ++i) {
+                const ses_solver* h = c.mem[i];
+                const bool m = mask && h->has_mask;
+                PassArgs<T>& a = host[((size_t)prog * 2 + mask) * nm + i];
+                if (prog < BP_NX) {
+                    const XProg p = batch_xprog(prog, m);
+                    a = make_args<T>(h, 0, h->psi, h->psi);
+                    a.d_load = p.d_load; a.d_mid = p.d_mid; a.d_store = p.d_store;
+                    a.m_load = p.m_load; a.m_mid = p.m_mid; a.m_store = p.m_store;
+                    a.out_scale = p.out_scale;
+                } else if (prog - BP_MID0 < c.nmid) {
+                    a = make_args<T>(h, c.mid_axis[prog - BP_MID0], h->psi, h->psi);
+                } else {
+                    a = make_args<T>(h, 0, h->psi, h->psi);  // unused slot
+                }
+            }
+    class_select<T>(b, c);
+    SES_TRY(class_maps(c, 0, c.dmaps, c.mcap));
+    const size_t bytes = host.size() * sizeof(PassArgs<T>);
+    if (bytes > c.dcap) {
+        if (c.dargs) cudaFree(c.dargs);
+        c.dargs = nullptr;
+        c.dcap = 0;
+        const cudaError_t e = cudaMalloc(&c.dargs, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SES_ENOMEM, "batch argument table allocation failed");
+        }
+        c.dcap = bytes;
+    }
+    SES_CU(cudaMemcpy(c.dargs, host.data(), bytes, cudaMemcpyHostToDevice));
+    return SES_OK;
+}
+
+// One batched pass of program `prog` over every member of the class.
+// args_ovr / maps_ovr (autotuning): the pass's per-member arguments and the
+// tensor-map table to use instead of the class's own.
+template <typename T>
+ses_status class_launch(const ses_batch_s* b, const BatchClass& c, int prog, bool mask, cudaStream_t s,
+                        const PassArgs<T>* args_ovr = nullptr, const CUtensorMap* maps_ovr = nullptr) {
+    const ses_solver* h0 = c.mem[0];
+    const int axis = prog < BP_NX ? 0 : c.mid_axis[prog - BP_MID0];
+    const int mode = prog < BP_NX ? batch_xprog(prog, mask).mode : c.mid_mode[prog - BP_MID0];
+    const PassPlan& pp = h0->pp[axis];
+    const auto* e = reinterpret_cast<const PlanEntry<T>*>(pp.cp);
+    const size_t nm = c.mem.size();
+    const PassArgs<T>* args =
+        args_ovr ? args_ovr : reinterpret_cast<const PassArgs<T>*>(c.dargs) + ((size_t)prog * 2 + (mask ? 1 : 0)) * nm;
+    const CUtensorMap* maps = maps_ovr ? maps_ovr : c.dmaps;
+    const int q = prog - BP_MID0;
+    if (axis == 0 ? c.xvar >= 0 && (mode == XM_START || mode == XM_MID || mode == XM_END)
+                  : c.svar[q] >= 0) {
+        const int n = h0->n[axis];
+        PipeArgs pa{};
+        pa.err = b->derr;
+        BatchWork w{};
+        if (axis == 0) {
+            const auto& v = e->xv[c.xvar];
+            w.bpi = (uint32_t)((pp.nlines + v.lpc - 1) / v.lpc);
+        } else {
+            const auto& v = e->sv[c.svar[q]];
+            w.bpi = (uint32_t)((pp.nlines + v.ls - 1) / v.ls);
+            pa.kind = axis == 1 ? 0 : 1;
+            pa.rows_per_box = n > 256 ? 256 : n;
+            pa.nbox = n / pa.rows_per_box;
+        }
+        if ((unsigned long long)w.bpi * nm >= (1ull << 31))
+            return fail(SES_EINVAL, "batch class too large: instances x tiles must stay below 2^31");
+        w.total = (uint32_t)(w.bpi * nm);
+        w.fbpi = make_fastdiv(w.bpi);
+        pa.ntiles = (int)w.total;
+        if (axis == 0) {
+            const auto& v = e->xv[c.xvar];
+            const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * v.bbps[mode]));
+            v.kb[mode]<<<grid, 32 * v.warps, v.smem[mode], s>>>(args, w, pa);
+        } else {
+            const auto& v = e->sv[c.svar[q]];
+            const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * v.bbps[mode]));
+            v.kb[mode]<<<grid, v.ls * (n / e->e), v.smem, s>>>(args, maps + (size_t)q * nm, w, pa);
+        }
+        const cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess)
+            return fail(SES_EDEVICE, std::string("batched pipelined pass launch: ") + cudaGetErrorString(err));
+        return SES_OK;
+    }
+    if ((unsigned long long)pp.cgrid * nm >= (1ull << 31))
+        return fail(SES_EINVAL, "batch class too large: instances x tiles must stay below 2^31");
+    BatchWork w{};
+    w.bpi = pp.cgrid;
+    w.total = (uint32_t)(pp.cgrid * nm);
+    w.fbpi = make_fastdiv(w.bpi);
+    if (axis == 0) {
+        const int bps = std::max(1, e->xb_bps[mode]);
+        const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * bps));
+        e->xb[mode]<<<grid, pp.cblock, 0, s>>>(args, w);
+    } else {
+        const int bps = std::max(1, e->sb_bps[mode]);
+        const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * bps));
+        e->sb[mode]<<<grid, pp.cblock, pp.csmem, s>>>(args, w);
+    }
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return fail(SES_EDEVICE, std::string("batched pass launch: ") + cudaGetErrorString(err));
+    return SES_OK;
+}
+
+template <typename T>
+ses_status class_unit(const ses_batch_s* b, const BatchClass& c, bool mask, cudaStream_t s) {
+    if (c.mem[0]->last_axis == 0) return class_launch<T>(b, c, BP_1DMID, mask, s);
+    SES_TRY(class_launch<T>(b, c, BP_XMID, mask, s));
+    for (int q = 0; q < c.nmid; ++q) SES_TRY(class_launch<T>(b, c, BP_MID0 + q, mask, s));
+    return SES_OK;
+}
+
+template <typename T>
+ses_status class_body(const ses_batch_s* b, BatchClass& c, bool mask) {
+    cudaGraphExec_t& ex = c.body[mask ? 1 : 0];
+    if (ex) return SES_OK;
+    if (!c.cap) SES_CU(cudaStreamCreateWithFlags(&c.cap, cudaStreamNonBlocking));
+    SES_CU(cudaStreamBeginCapture(c.cap, cudaStreamCaptureModeThreadLocal));
+    ses_status st = SES_OK;
+    for (int u = 0; u < kBodyUnroll && st == SES_OK; ++u) st = class_unit<T>(b, c, mask, c.cap);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c.cap, &graph);
+    if (st != SES_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (e != cudaSuccess) return fail(SES_EDEVICE, std::string("graph capture: ") + cudaGetErrorString(e));
+    const cudaError_t ie = cudaGraphInstantiate(&ex, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+        ex = nullptr;
+        return fail(SES_EDEVICE, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    return SES_OK;
+}
+
+// S merged Strang steps of every member of a batched class, on stream s.
+template <typename T>
+ses_status class_steps(const ses_batch_s* b, BatchClass& c, int S, bool mask, cudaStream_t s) {
+    const bool one_d = c.mem[0]->last_axis == 0;
+    int interior;
+    if (one_d) {
+        if (S == 1) return class_launch<T>(b, c, BP_1DONE, mask, s);
+        SES_TRY(class_launch<T>(b, c, BP_1DFIRST, mask, s));
+        interior = S - 2;
+    } else {
+        SES_TRY(class_launch<T>(b, c, BP_XSTART, mask, s));
+        for (int q = 0; q < c.nmid; ++q) SES_TRY(class_launch<T>(b, c, BP_MID0 + q, mask, s));
+        interior = S - 1;
+    }
+    if (interior >= kBodyUnroll) SES_TRY(class_body<T>(b, c, mask));
+    while (interior >= kBodyUnroll) {
+        SES_CU(cudaGraphLaunch(c.body[mask ? 1 : 0], s));
+        interior -= kBodyUnroll;
+    }
+    for (; interior > 0; --interior) SES_TRY(class_unit<T>(b, c, mask, s));
+    return class_launch<T>(b, c, one_d ? BP_1DLAST : BP_XEND, mask, s);
+}
+
+// Regroup members into classes and refresh the argument tables of changed ones.
+ses_status batch_refresh(ses_batch_s* b) {
+    bool any_dirty = false;
+    for (BatchClass* c : b->classes) any_dirty |= c->dirty;
+    if (!any_dirty) return SES_OK;
+    SES_TRY(batch_wait(b, 0));  // no launch in flight reads the tables being replaced
+    for (BatchClass* c : b->classes) {
+        if (!c->dirty || c->mem.empty()) continue;
+        for (auto& g : c->body) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+        SES_TRY(c->prec == SES_C128 ? class_upload<double>(b, *c) : class_upload<float>(b, *c));
+        if (!c->cs) SES_CU(cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking));
+        if (!c->done) SES_CU(cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming));
+        c->dirty = false;
+    }
+    return SES_OK;
+}
+
+BatchClass* find_class(ses_batch_s* b, const ses_solver* h) {
+    for (BatchClass* c : b->classes)
+        if (c->prec == h->prec && c->n[0] == h->n[0] && c->n[1] == h->n[1] && c->n[2] == h->n[2]) return c;
+    return nullptr;
+}
+
+// Times every variant of each class pass on the members' scratch fields (psi is
+// not touched) and keeps the fastest in b->sel.
+template <typename T>
+ses_status class_autotune(ses_batch_s* b, BatchClass& c, std::map<std::string, int>& chosen) {
+    const size_t nm = c.mem.size();
+    const ses_solver* h0 = c.mem[0];
+    if (!c.batched || h0->last_axis == 0) return SES_OK;
+    std::vector<PassArgs<T>> host(nm * (1 + (size_t)c.nmid));
+    for (size_t i = 0; i < nm; ++i) {
+        const ses_solver* h = c.mem[i];
+        PassArgs<T>& a = host[i];
+        const XProg p = batch_xprog(BP_XMID, h->has_mask);
+        a = make_args<T>(h, 0, h->scratch, h->scratch);
+        a.d_mid = p.d_mid;
+        a.m_mid = p.m_mid;
+        for (int q = 0; q < c.nmid; ++q) host[(1 + (size_t)q) * nm + i] = make_args<T>(h, c.mid_axis[q], h->scratch, h->scratch);
+    }
+    PassArgs<T>* dargs = nullptr;
+    CUtensorMap* dmaps = nullptr;
+    size_t mcap = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ses_status st = SES_OK;
+    auto cleanup = [&]() {
+        if (dargs) cudaFree(dargs);
+        if (dmaps) cudaFree(dmaps);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    };
+    if (cudaMalloc(&dargs, host.size() * sizeof(PassArgs<T>)) != cudaSuccess ||
+        cudaMemcpy(dargs, host.data(), host.size() * sizeof(PassArgs<T>), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        return fail(SES_ENOMEM, "batch autotune buffers");
+    }
+    const int saved_x = c.xvar;
+    int saved_s[3] = {c.svar[0], c.svar[1], c.svar[2]};
+    auto time_prog = [&](int prog, float* ms) -> ses_status {
+        const PassArgs<T>* a = dargs + (prog == BP_XMID ? 0 : (size_t)(1 + prog - BP_MID0) * nm);
+        SES_TRY(class_maps(c, 1, dmaps, mcap));
+        SES_TRY(class_launch<T>(b, c, prog, true, b->stream, a, dmaps));
+        SES_CU(cudaEventRecord(e0, b->stream));
+        for (int r = 0; r < 3; ++r) SES_TRY(class_launch<T>(b, c, prog, true, b->stream, a, dmaps));
+        SES_CU(cudaEventRecord(e1, b->stream));
+        SES_TRY(batch_wait(b, 60000));
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        *ms = t / 3;
+        return SES_OK;
+    };
+    // x pass between steps
+    {
+        const auto* ex = reinterpret_cast<const PlanEntry<T>*>(h0->pp[0].cp);
+        int best = -1;
+        float best_ms = 1e30f;
+        for (int k = -1; k < (int)ex->xv.size() && st == SES_OK; ++k) {
+            if (k >= 0 && !xvar_ok<T>(c, k)) continue;
+            c.xvar = k;
+            float ms = 0.f;
+            st = time_prog(BP_XMID, &ms);
+            if (st == SES_OK && ms < best_ms) {
+                best_ms = ms;
+                best = k;
+            }
+        }
+        c.xvar = saved_x;
+        if (st == SES_OK) chosen[batch_tune_key(b, c, 0)] = best;
+    }
+    for (int q = 0; q < c.nmid && st == SES_OK; ++q) {
+        const auto* es = reinterpret_cast<const PlanEntry<T>*>(h0->pp[c.mid_axis[q]].cp);
+        int best = -1;
+        float best_ms = 1e30f;
+        for (int k = -1; k < (int)es->sv.size() && st == SES_OK; ++k) {
+            if (k >= 0 && !(svar_ok<T>(c, q, k, 1) && svar_ok<T>(c, q, k, 0))) continue;
+            c.svar[q] = k;
+            float ms = 0.f;
+            st = time_prog(BP_MID0 + q, &ms);
+            if (st == SES_OK && ms < best_ms) {
+                best_ms = ms;
+                best = k;
+            }
+        }
+        c.svar[q] = saved_s[q];
+        if (st == SES_OK) chosen[batch_tune_key(b, c, 1 + q)] = best;
+    }
+    cleanup();
+    return st;
+}
+
+ses_status batch_remove_impl(ses_batch_s* b, ses_solver* h) {
+    auto it = std::find(b->members.begin(), b->members.end(), h);
+    if (it == b->members.end()) return fail(SES_ENOTFOUND, "handle is not a member of this batch");
+    SES_TRY(batch_wait(b, 0));
+    b->members.erase(it);
+    BatchClass* c = find_class(b, h);
+    if (c) {
+        c->mem.erase(std::find(c->mem.begin(), c->mem.end(), h));
+        c->dirty = true;
+        if (c->mem.empty()) {
+            b->classes.erase(std::find(b->classes.begin(), b->classes.end(), c));
+            drop_class(c);
+        }
+    }
+    h->batch = nullptr;
+    h->stream = h->own;
+    return SES_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1230,6 +1774,7 @@ ses_status ses_gpu_create(const ses_grid_desc* grid, ses_precision prec, double 
 
 ses_status ses_gpu_destroy(ses_handle h) {
     SES_TRY(check_handle(h));
+    if (h->batch) SES_TRY(batch_remove_impl(h->batch, h));
     release(h);
     return SES_OK;
 }
@@ -1368,22 +1913,7 @@ ses_status ses_gpu_observe(ses_handle h, double xlo, double xhi, ses_observables
     SES_TRY(h->prec == SES_C128 ? enqueue_observe<double>(h, xlo, xhi)
                                 : enqueue_observe<float>(h, xlo, xhi));
     SES_TRY(wait_bounded(h, 0));
-    const double* r = h->hsums;
-    const double* k = h->hsums + kRedR;
-    const double dv = ((h->box[1] - h->box[0]) / h->n[0]) * ((h->box[3] - h->box[2]) / h->n[1]) *
-                      ((h->box[5] - h->box[4]) / h->n[2]);
-    auto ratio = [](double num, double den) { return den > 0.0 ? num / den : 0.0; };
-    out->norm = r[0] * dv;
-    out->energy_v = ratio(r[1], r[0]);
-    out->energy_t = ratio(k[1], k[0]);
-    out->energy = out->energy_v + out->energy_t;
-    out->p_range = r[2] * dv;
-    for (int a = 0; a < 3; ++a) {
-        out->mean_pos[a] = ratio(r[3 + a], r[0]);
-        const double var = ratio(r[6 + a], r[0]) - out->mean_pos[a] * out->mean_pos[a];
-        out->sigma_pos[a] = std::sqrt(std::max(0.0, var));
-        out->mean_mom[a] = ratio(k[2 + a], k[0]);
-    }
+    finish_observe(h, out);
     return SES_OK;
 }
 
@@ -1437,6 +1967,7 @@ ses_status ses_gpu_sync(ses_handle h, int timeout_ms) {
 
 ses_status ses_gpu_set_stream(ses_handle h, void* cuda_stream) {
     SES_TRY(check_handle(h));
+    if (h->batch) return fail(SES_EBUSY, "handle belongs to a batch; set the batch's stream instead");
     SES_TRY(wait_bounded(h, 0));
     h->stream = cuda_stream ? reinterpret_cast<cudaStream_t>(cuda_stream) : h->own;
     return SES_OK;
@@ -1493,6 +2024,235 @@ ses_status ses_fft3_host(const int32_t* n, ses_precision prec, double* data, int
     if (st == SES_OK) st = ses_gpu_read_psi(h, data);
     release(h);
     return st;
+}
+
+
+// ---------------------------------------------------------------------------
+// Batches
+// ---------------------------------------------------------------------------
+static ses_status check_batch(ses_batch b) {
+    if (!b) return fail(SES_EINVAL, "null batch");
+    return SES_OK;
+}
+
+ses_status ses_batch_create(ses_batch* out) {
+    if (!out) return fail(SES_EINVAL, "null output");
+    *out = nullptr;
+    ses_batch_s* b = new ses_batch_s();
+    cudaGetDevice(&b->dev);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->dev);
+    if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (b->fork) cudaEventDestroy(b->fork);
+        if (b->own) cudaStreamDestroy(b->own);
+        delete b;
+        return fail(SES_EDEVICE, "batch stream creation failed (no device?)");
+    }
+    if (cudaMalloc(&b->derr, sizeof(unsigned)) != cudaSuccess ||
+        cudaMallocHost(&b->herr, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(b->derr, 0, sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        if (b->derr) cudaFree(b->derr);
+        cudaEventDestroy(b->ev);
+        cudaEventDestroy(b->fork);
+        cudaStreamDestroy(b->own);
+        delete b;
+        return fail(SES_ENOMEM, "batch error word allocation failed");
+    }
+    *b->herr = 0;
+    b->stream = b->own;
+    *out = b;
+    return SES_OK;
+}
+
+ses_status ses_batch_destroy(ses_batch b) {
+    SES_TRY(check_batch(b));
+    const ses_status st = batch_wait(b, 0);
+    for (ses_solver* h : b->members) {
+        h->batch = nullptr;
+        h->stream = h->own;
+    }
+    for (BatchClass* c : b->classes) drop_class(c);
+    if (b->derr) cudaFree(b->derr);
+    if (b->herr) cudaFreeHost(b->herr);
+    if (b->ev) cudaEventDestroy(b->ev);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->own) cudaStreamDestroy(b->own);
+    delete b;
+    return st;
+}
+
+ses_status ses_batch_add(ses_batch b, ses_handle h) {
+    SES_TRY(check_batch(b));
+    SES_TRY(check_handle(h));
+    if (h->batch) return fail(SES_EBUSY, "handle already belongs to a batch");
+    if (!h->with_tables) return fail(SES_EINVAL, "handle has no phase tables");
+    if (h->dev != b->dev) return fail(SES_EINVAL, "handle and batch are on different devices");
+    SES_TRY(wait_bounded(h, 0));
+    h->batch = b;
+    h->stream = b->stream;
+    b->members.push_back(h);
+    BatchClass* c = find_class(b, h);
+    if (!c) {
+        c = new BatchClass();
+        c->prec = h->prec;
+        for (int a = 0; a < 3; ++a) c->n[a] = h->n[a];
+        b->classes.push_back(c);
+    }
+    c->mem.push_back(h);
+    c->dirty = true;
+    return SES_OK;
+}
+
+ses_status ses_batch_remove(ses_batch b, ses_handle h) {
+    SES_TRY(check_batch(b));
+    SES_TRY(check_handle(h));
+    if (h->batch != b) return fail(SES_ENOTFOUND, "handle is not a member of this batch");
+    return batch_remove_impl(b, h);
+}
+
+ses_status ses_batch_step(ses_batch b, int nsteps, int absorb) {
+    SES_TRY(check_batch(b));
+    if (nsteps < 0) return fail(SES_EINVAL, "nsteps must be >= 0");
+    if (nsteps == 0 || b->members.empty()) return SES_OK;
+    SES_TRY(batch_refresh(b));
+    const bool mask = absorb != 0;
+    SES_CU(cudaEventRecord(b->fork, b->stream));
+    for (BatchClass* c : b->classes) {
+        if (!c->batched) {  // no batched kernels for this shape: each member steps on the batch stream
+            for (ses_solver* h : c->mem) SES_TRY(ses_gpu_step(h, nsteps, absorb));
+            continue;
+        }
+        SES_CU(cudaStreamWaitEvent(c->cs, b->fork, 0));
+        SES_TRY(c->prec == SES_C128 ? class_steps<double>(b, *c, nsteps, mask, c->cs)
+                                    : class_steps<float>(b, *c, nsteps, mask, c->cs));
+        SES_CU(cudaEventRecord(c->done, c->cs));
+        SES_CU(cudaStreamWaitEvent(b->stream, c->done, 0));
+    }
+    return SES_OK;
+}
+
+ses_status ses_batch_observe(ses_batch b, double xlo, double xhi, ses_observables* out, int count) {
+    SES_TRY(check_batch(b));
+    if (!out && count) return fail(SES_EINVAL, "null output");
+    if (count != (int)b->members.size())
+        return fail(SES_EINVAL, "count must equal the number of members (" +
+                                    std::to_string(b->members.size()) + ")");
+    for (ses_solver* h : b->members)
+        SES_TRY(h->prec == SES_C128 ? enqueue_observe<double>(h, xlo, xhi) : enqueue_observe<float>(h, xlo, xhi));
+    SES_TRY(batch_wait(b, 0));
+    for (int i = 0; i < count; ++i) finish_observe(b->members[i], &out[i]);
+    return SES_OK;
+}
+
+ses_status ses_batch_autotune(ses_batch b, int flags) {
+    SES_TRY(check_batch(b));
+    SES_TRY(batch_refresh(b));
+    std::map<std::string, int> chosen;
+    for (BatchClass* c : b->classes)
+        SES_TRY(c->prec == SES_C128 ? class_autotune<double>(b, *c, chosen) : class_autotune<float>(b, *c, chosen));
+    for (const auto& kv : chosen) b->sel[kv.first] = kv.second;
+    for (BatchClass* c : b->classes) c->dirty = true;  // re-select, re-upload maps, re-capture graphs
+    if (flags & 1) write_tune_cache(chosen);
+    return batch_refresh(b);
+}
+
+ses_status ses_batch_info(ses_batch b, char* buf, size_t len) {
+    SES_TRY(check_batch(b));
+    if (!buf || len == 0) return fail(SES_EINVAL, "null buffer");
+    SES_TRY(batch_refresh(b));
+    std::ostringstream o;
+    for (size_t i = 0; i < b->classes.size(); ++i) {
+        const BatchClass* c = b->classes[i];
+        o << (i ? "; " : "") << c->n[0] << "x" << c->n[1] << "x" << c->n[2] << " "
+          << (c->prec == SES_C128 ? "c128" : "c64") << " members=" << c->mem.size();
+        if (!c->batched) {
+            o << " member-by-member";
+            continue;
+        }
+        o << " x=" << (c->xvar >= 0 ? "pipe" + std::to_string(c->xvar) : std::string("reg"));
+        for (int q = 0; q < c->nmid; ++q)
+            o << " s" << q << "=" << (c->svar[q] >= 0 ? "pipe" + std::to_string(c->svar[q]) : std::string("reg"));
+    }
+    const std::string t = o.str();
+    std::snprintf(buf, len, "%s", t.c_str());
+    return SES_OK;
+}
+
+ses_status ses_batch_sync(ses_batch b, int timeout_ms) {
+    SES_TRY(check_batch(b));
+    return batch_wait(b, timeout_ms);
+}
+
+ses_status ses_batch_set_stream(ses_batch b, void* cuda_stream) {
+    SES_TRY(check_batch(b));
+    SES_TRY(batch_wait(b, 0));
+    b->stream = cuda_stream ? reinterpret_cast<cudaStream_t>(cuda_stream) : b->own;
+    for (ses_solver* h : b->members) h->stream = b->stream;
+    return SES_OK;
+}
+
+ses_status ses_batch_members(ses_batch b, int* members, int* classes) {
+    SES_TRY(check_batch(b));
+    if (members) *members = (int)b->members.size();
+    if (classes) *classes = (int)b->classes.size();
+    return SES_OK;
+}
+
+ses_status ses_batch_profile(ses_batch b, int nsteps, int absorb, double* ms, int count) {
+    SES_TRY(check_batch(b));
+    if (nsteps < 1) return fail(SES_EINVAL, "nsteps must be >= 1");
+    if (!ms || count < (int)b->classes.size() * 5)
+        return fail(SES_EINVAL, "output needs 5 values per class");
+    SES_TRY(batch_refresh(b));
+    const bool mask = absorb != 0;
+    for (size_t ci = 0; ci < b->classes.size(); ++ci) {
+        BatchClass* c = b->classes[ci];
+        double* o = ms + 5 * ci;
+        for (int q = 0; q < 5; ++q) o[q] = 0.0;
+        if (!c->batched) continue;
+        const bool one_d = c->mem[0]->last_axis == 0;
+        std::vector<int> progs;
+        progs.push_back(one_d ? (int)BP_1DMID : (int)BP_XMID);
+        if (!one_d)
+            for (int q = 0; q < c->nmid; ++q) progs.push_back(BP_MID0 + q);
+        std::vector<cudaEvent_t> ev((size_t)nsteps * progs.size() + 1);
+        for (auto& e : ev) SES_CU(cudaEventCreate(&e));
+        size_t k = 0;
+        auto run = [&](int prog) {
+            return c->prec == SES_C128 ? class_launch<double>(b, *c, prog, mask, b->stream)
+                                       : class_launch<float>(b, *c, prog, mask, b->stream);
+        };
+        // untimed batch start, so that the fields stay a valid Strang batch
+        ses_status st = run(one_d ? (int)BP_1DFIRST : (int)BP_XSTART);
+        if (!one_d)
+            for (int q = 0; q < c->nmid && st == SES_OK; ++q) st = run(BP_MID0 + q);
+        if (st == SES_OK) SES_CU(cudaEventRecord(ev[k++], b->stream));
+        for (int s = 0; s < nsteps && st == SES_OK; ++s)
+            for (int prog : progs) {
+                st = c->prec == SES_C128 ? class_launch<double>(b, *c, prog, mask, b->stream)
+                                         : class_launch<float>(b, *c, prog, mask, b->stream);
+                if (st != SES_OK) break;
+                cudaEventRecord(ev[k++], b->stream);
+            }
+        if (st == SES_OK) st = run(one_d ? (int)BP_1DLAST : (int)BP_XEND);
+        if (st == SES_OK) st = batch_wait(b, 0);
+        if (st == SES_OK) {
+            for (int s = 0; s < nsteps; ++s)
+                for (size_t p = 0; p < progs.size(); ++p) {
+                    const size_t i = 1 + (size_t)s * progs.size() + p;
+                    float t = 0.f;
+                    cudaEventElapsedTime(&t, ev[i - 1], ev[i]);
+                    o[p] += t / nsteps;
+                    o[4] += t / nsteps;
+                }
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        if (st != SES_OK) return st;
+    }
+    return SES_OK;
 }
 
 }  // extern "C"

@@ -142,8 +142,11 @@ struct XShape {
     static constexpr int NW = (48 * 1024) / per_warp >= 4 ? 4 : ((48 * 1024) / per_warp < 1 ? 1 : (48 * 1024) / per_warp);
 };
 
-template <typename T, int MODE, int N, int E, int R0, int R1, int R2>
-__global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4) xpass2_kernel(const PassArgs<T> a) {
+// Body of the contiguous pass for CTA tile `blk` (NW * LPW lines); `a` is the
+// kernel parameter (single field) or an entry of a per-instance array in
+// global memory (batched passes).
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, class A>
+__device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb) {
     using XS = XShape<T, N, E>;
     constexpr int TL = XS::TL;
     constexpr int LPW = XS::LPW;
@@ -151,10 +154,9 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4) xpass2_kernel(con
     constexpr int NW = XS::NW;
     using S = PlanShape<R0, R1, R2>;
     constexpr int RF = R0, RL = S::last;
-    __shared__ cx<T> xb[NW * LPW * PITCH];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int lw = lane / TL, q = lane % TL;
-    const long long m = ((long long)blockIdx.x * NW + warp) * LPW + lw;
+    const long long m = (blk * NW + warp) * LPW + lw;
     const bool valid = m < a.nlines;
     const long long mc = valid ? m : 0;
     const int kz = (int)fdiv((uint32_t)mc, a.fny);
@@ -256,19 +258,24 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4) xpass2_kernel(con
     }
 }
 
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2>
+__global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4) xpass2_kernel(const PassArgs<T> a) {
+    using XS = XShape<T, N, E>;
+    __shared__ cx<T> xb[XS::NW * XS::LPW * XS::PITCH];
+    xpass2_body<T, MODE, N, E, R0, R1, R2>(a, (long long)blockIdx.x, xb);
+}
+
 // ---------------------------------------------------------------------------
 // Strided-axis (y or z) pass, compiled plan.  CTA = L lines x N/E threads per
 // line; thread (l = tid % L, q = tid / L).  Modes as in SModeK.
 // ---------------------------------------------------------------------------
-template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L>
-__global__ void __launch_bounds__(L*(N / E), 1) spass2_kernel(const PassArgs<T> a) {
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, class A>
+__device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* tile) {
     constexpr int TL = N / E;
     using S = PlanShape<R0, R1, R2>;
     constexpr int RL = S::last;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    cx<T>* tile = reinterpret_cast<cx<T>*>(smraw);
     const int l = threadIdx.x % L, q = threadIdx.x / L;
-    const long long s = (long long)blockIdx.x * L + l;
+    const long long s = blk * L + l;
     const bool valid = s < a.nlines;
     const long long sc_ = valid ? s : 0;
     const long long w = (long long)fdiv((uint32_t)sc_, a.fnu);
@@ -354,6 +361,46 @@ __global__ void __launch_bounds__(L*(N / E), 1) spass2_kernel(const PassArgs<T> 
                     a.dst[base + pos * se] = cconj(v[b * R0 + r]);
                 }
         }
+    }
+}
+
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L>
+__global__ void __launch_bounds__(L*(N / E), 1) spass2_kernel(const PassArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    spass2_body<T, MODE, N, E, R0, R1, R2, L>(a, (long long)blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
+}
+
+// ---------------------------------------------------------------------------
+// Batched passes: the same bodies over many fields of one shape, one launch.
+// Work item t is tile (t mod bpi) of instance t / bpi; each instance has its
+// own PassArgs (field, potential table, axis tables) in global memory.  CTAs
+// walk the items with a grid stride; the grid is sized to the resident CTAs.
+// ---------------------------------------------------------------------------
+struct BatchWork {
+    uint32_t total;  // instances x tiles per instance
+    uint32_t bpi;    // tiles per instance
+    FastDiv fbpi;
+};
+
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2>
+__global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4)
+    xbatch_kernel(const PassArgs<T>* __restrict__ args, const BatchWork w) {
+    using XS = XShape<T, N, E>;
+    __shared__ cx<T> xb[XS::NW * XS::LPW * XS::PITCH];
+    for (uint32_t t = blockIdx.x; t < w.total; t += gridDim.x) {
+        const uint32_t inst = fdiv(t, w.fbpi);
+        xpass2_body<T, MODE, N, E, R0, R1, R2>(args[inst], (long long)(t - inst * w.bpi), xb);
+    }
+}
+
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L>
+__global__ void __launch_bounds__(L*(N / E), 1)
+    sbatch_kernel(const PassArgs<T>* __restrict__ args, const BatchWork w) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T>* tile = reinterpret_cast<cx<T>*>(smraw);
+    for (uint32_t t = blockIdx.x; t < w.total; t += gridDim.x) {
+        const uint32_t inst = fdiv(t, w.fbpi);
+        spass2_body<T, MODE, N, E, R0, R1, R2, L>(args[inst], (long long)(t - inst * w.bpi), tile);
     }
 }
 

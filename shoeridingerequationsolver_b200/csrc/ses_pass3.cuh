@@ -42,12 +42,35 @@ __device__ __forceinline__ void pipe_abort(const PipeArgs& pa, const uint64_t* b
         (void)mbar_wait(smem_u32(&bars[j % nbuf]), (uint32_t)((j / nbuf) & 1));
 }
 
+// Where a pipelined pass finds the tile with global index t (t walks
+// blockIdx.x, blockIdx.x + gridDim.x, ...): one field (kernel parameters) or
+// many fields of one shape (per-instance arguments and tensor maps in global
+// memory; tile t is tile t mod bpi of instance t / bpi).
+template <typename T>
+struct OneField {
+    const PassArgs<T>& a;
+    const CUtensorMap* map;
+    __device__ __forceinline__ const PassArgs<T>& args(uint32_t) const { return a; }
+    __device__ __forceinline__ long long local(uint32_t t) const { return (long long)t; }
+    __device__ __forceinline__ const CUtensorMap* tmap(uint32_t) const { return map; }
+};
+
+template <typename T>
+struct ManyFields {
+    const PassArgs<T>* __restrict__ arr;
+    const CUtensorMap* maps;
+    BatchWork w;
+    __device__ __forceinline__ uint32_t inst(uint32_t t) const { return fdiv(t, w.fbpi); }
+    __device__ __forceinline__ const PassArgs<T>& args(uint32_t t) const { return arr[inst(t)]; }
+    __device__ __forceinline__ long long local(uint32_t t) const { return (long long)(t - inst(t) * w.bpi); }
+    __device__ __forceinline__ const CUtensorMap* tmap(uint32_t t) const { return maps + inst(t); }
+};
+
 // ---------------------------------------------------------------------------
 // Strided axis (y or z).  CTA = L lines x N/E threads; tile = N rows x L lines.
 // ---------------------------------------------------------------------------
-template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, int NBUF, int MINB>
-__global__ void __launch_bounds__(L*(N / E), MINB)
-    spass3_kernel(const PassArgs<T> a, const __grid_constant__ CUtensorMap tmap, const PipeArgs pa) {
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, int NBUF, class F>
+__device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
     constexpr int TL = N / E;
     constexpr int EW = (int)sizeof(cx<T>) / 8;  // 8-byte words per element
     constexpr uint32_t TILE_BYTES = (uint32_t)(N * L * sizeof(cx<T>));
@@ -66,22 +89,24 @@ __global__ void __launch_bounds__(L*(N / E), MINB)
     __syncthreads();
     auto issue = [&](int i) {  // thread 0: load this CTA's i-th tile into buffer i % NBUF
         const int buf = i % NBUF;
-        const long long s0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * L;
+        const uint32_t t = blockIdx.x + (uint32_t)i * gridDim.x;
+        const long long s0 = f.local(t) * L;
+        const long long nx = f.args(t).nx;
+        const CUtensorMap* map = f.tmap(t);
         const uint32_t bar = smem_u32(&bars[buf]);
         const uint32_t dst = smem_u32(tiles + (size_t)buf * N * L);
         mbar_expect_tx(bar, TILE_BYTES);
         for (int bx = 0; bx < pa.nbox; ++bx) {
             const uint32_t d = dst + (uint32_t)(bx * pa.rows_per_box * L * (int)sizeof(cx<T>));
             if (pa.kind == 0)
-                tma_load_3d(d, &tmap, (int)(s0 % a.nx) * EW, bx * pa.rows_per_box, (int)(s0 / a.nx), bar);
+                tma_load_3d(d, map, (int)(s0 % nx) * EW, bx * pa.rows_per_box, (int)(s0 / nx), bar);
             else
-                tma_load_2d(d, &tmap, (int)s0 * EW, bx * pa.rows_per_box, bar);
+                tma_load_2d(d, map, (int)s0 * EW, bx * pa.rows_per_box, bar);
         }
     };
     if (threadIdx.x == 0)
         for (int i = 0; i < NBUF && i < nmine; ++i) issue(i);
 
-    const bool ypass = a.axis == 1;
     for (int i = 0; i < nmine; ++i) {
         const int buf = i % NBUF;
         const bool ok = mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i / NBUF) & 1));
@@ -89,8 +114,11 @@ __global__ void __launch_bounds__(L*(N / E), MINB)
             pipe_abort(pa, bars, NBUF, i, nmine);
             return;
         }
+        const uint32_t t = blockIdx.x + (uint32_t)i * gridDim.x;
+        const PassArgs<T>& a = f.args(t);
+        const bool ypass = a.axis == 1;
         cx<T>* tile = tiles + (size_t)buf * N * L;
-        const long long s = (long long)((int)blockIdx.x + i * (int)gridDim.x) * L + l;
+        const long long s = f.local(t) * L + l;
         const bool valid = s < a.nlines;
         const long long sc_ = valid ? s : 0;
         const long long w = (long long)fdiv((uint32_t)sc_, a.fnu);
@@ -158,6 +186,20 @@ __global__ void __launch_bounds__(L*(N / E), MINB)
     }
 }
 
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, int NBUF, int MINB>
+__global__ void __launch_bounds__(L*(N / E), MINB)
+    spass3_kernel(const PassArgs<T> a, const __grid_constant__ CUtensorMap tmap, const PipeArgs pa) {
+    spass3_body<T, MODE, N, E, R0, R1, R2, L, NBUF>(OneField<T>{a, &tmap}, pa);
+}
+
+// Batched: the fields of one shape class, per-instance tensor maps in global memory.
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, int NBUF, int MINB>
+__global__ void __launch_bounds__(L*(N / E), MINB)
+    sbatch3_kernel(const PassArgs<T>* __restrict__ args, const CUtensorMap* maps, const BatchWork w,
+                   const PipeArgs pa) {
+    spass3_body<T, MODE, N, E, R0, R1, R2, L, NBUF>(ManyFields<T>{args, maps, w}, pa);
+}
+
 // ---------------------------------------------------------------------------
 // Contiguous axis (x).  NW warps per CTA, a warp owns 32/(N/E) lines; a tile
 // is the CTA's consecutive lines, copied whole (plus the potential-table rows
@@ -168,8 +210,8 @@ struct XUsesTable {
     static constexpr bool value = MODE == XM_START || MODE == XM_MID || MODE == XM_END || MODE == XM_1D;
 };
 
-template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int NW, int NBUF, int MINB>
-__global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T> a, const PipeArgs pa) {
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int NW, int NBUF, class F>
+__device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
     constexpr int TL = N / E;
     constexpr int LPW = 32 / TL;
     constexpr int LPC = NW * LPW;
@@ -183,7 +225,6 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int lw = lane / TL, q = lane % TL;
     const int nmine = blockIdx.x < (unsigned)pa.ntiles ? (pa.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-    const cx<T>* vtab = reinterpret_cast<const cx<T>*>(a.tb.vtab);
 
     if (threadIdx.x == 0) {
         for (int b = 0; b < NBUF; ++b) mbar_init(smem_u32(&bars[b]), 1);
@@ -192,7 +233,10 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
     __syncthreads();
     auto issue = [&](int i) {
         const int buf = i % NBUF;
-        const long long m0 = (long long)((int)blockIdx.x + i * (int)gridDim.x) * LPC;
+        const uint32_t t = blockIdx.x + (uint32_t)i * gridDim.x;
+        const PassArgs<T>& a = f.args(t);
+        const cx<T>* vtab = reinterpret_cast<const cx<T>*>(a.tb.vtab);
+        const long long m0 = f.local(t) * LPC;
         const long long rem = a.nlines - m0;
         const int nval = rem < LPC ? (int)rem : LPC;
         const uint32_t bytes = (uint32_t)(nval * N * (int)sizeof(cx<T>));
@@ -212,10 +256,12 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
             pipe_abort(pa, bars, NBUF, i, nmine);
             return;
         }
+        const uint32_t t = blockIdx.x + (uint32_t)i * gridDim.x;
+        const PassArgs<T>& a = f.args(t);
         cx<T>* ptile = reinterpret_cast<cx<T>*>(smraw3 + (size_t)buf * BUF_BYTES);
         const cx<T>* ttile = reinterpret_cast<const cx<T>*>(smraw3 + (size_t)buf * BUF_BYTES + PSI_BYTES);
         const int lc = warp * LPW + lw;  // line within the tile
-        const long long m = (long long)((int)blockIdx.x + i * (int)gridDim.x) * LPC + lc;
+        const long long m = f.local(t) * LPC + lc;
         const bool valid = m < a.nlines;
         const long long mc = valid ? m : 0;
         const int kz = (int)fdiv((uint32_t)mc, a.fny);
@@ -308,6 +354,17 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
         __syncthreads();
         if (threadIdx.x == 0 && i + NBUF < nmine) issue(i + NBUF);
     }
+}
+
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int NW, int NBUF, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T> a, const PipeArgs pa) {
+    xpass3_body<T, MODE, N, E, R0, R1, R2, NW, NBUF>(OneField<T>{a, nullptr}, pa);
+}
+
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int NW, int NBUF, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB)
+    xbatch3_kernel(const PassArgs<T>* __restrict__ args, const BatchWork w, const PipeArgs pa) {
+    xpass3_body<T, MODE, N, E, R0, R1, R2, NW, NBUF>(ManyFields<T>{args, nullptr, w}, pa);
 }
 
 }  // namespace sesk

@@ -23,20 +23,33 @@ struct PlanEntry {
     // pipelined variants; the solver picks one per axis (default 0, or autotuned)
     using XPipe = void (*)(const PassArgs<T>, const PipeArgs);
     using SPipe = void (*)(const PassArgs<T>, const CUtensorMap, const PipeArgs);
+    // batched forms: per-instance arguments (and tensor maps) in global memory
+    using XBPipe = void (*)(const PassArgs<T>*, const BatchWork, const PipeArgs);
+    using SBPipe = void (*)(const PassArgs<T>*, const CUtensorMap*, const BatchWork, const PipeArgs);
     struct XVar {
         XPipe k[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+        XBPipe kb[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
         int warps = 0, lpc = 0, nbuf = 0;
         size_t smem[7] = {0, 0, 0, 0, 0, 0, 0};
         int bps[7] = {0, 0, 0, 0, 0, 0, 0};  // resident CTAs per SM
+        int bbps[7] = {0, 0, 0, 0, 0, 0, 0};
     };
     struct SVar {
         SPipe k[4] = {nullptr, nullptr, nullptr, nullptr};
+        SBPipe kb[4] = {nullptr, nullptr, nullptr, nullptr};
         int ls = 0, nbuf = 0;
         size_t smem = 0;
         int bps[4] = {0, 0, 0, 0};
+        int bbps[4] = {0, 0, 0, 0};
     };
     std::vector<XVar> xv;
     std::vector<SVar> sv;
+    // batched kernels (many fields of this length per launch), by mode
+    using XBatch = void (*)(const PassArgs<T>*, const BatchWork);
+    XBatch xb[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    XBatch sb[4] = {nullptr, nullptr, nullptr, nullptr};
+    int xb_bps[7] = {0, 0, 0, 0, 0, 0, 0};  // resident CTAs per SM
+    int sb_bps[4] = {0, 0, 0, 0};
 };
 
 template <typename K>
@@ -67,6 +80,24 @@ PlanEntry<T> make_plan_entry() {
     p.sk[SM_REDUCE] = spass2_kernel<T, SM_REDUCE, N, E, R0, R1, R2, LS>;
     const int smem = N * LS * (int)sizeof(cx<T>);
     for (auto k : p.sk) allow_smem(k, smem);
+    p.xb[XM_START] = xbatch_kernel<T, XM_START, N, E, R0, R1, R2>;
+    p.xb[XM_MID] = xbatch_kernel<T, XM_MID, N, E, R0, R1, R2>;
+    p.xb[XM_END] = xbatch_kernel<T, XM_END, N, E, R0, R1, R2>;
+    p.xb[XM_1D] = xbatch_kernel<T, XM_1D, N, E, R0, R1, R2>;
+    p.sb[SM_FWD] = sbatch_kernel<T, SM_FWD, N, E, R0, R1, R2, LS>;
+    p.sb[SM_INV] = sbatch_kernel<T, SM_INV, N, E, R0, R1, R2, LS>;
+    p.sb[SM_FUSED] = sbatch_kernel<T, SM_FUSED, N, E, R0, R1, R2, LS>;
+    for (int m = 0; m < 7; ++m)
+        if (p.xb[m])
+            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&p.xb_bps[m], p.xb[m], p.xw * 32, 0,
+                                                                  cudaOccupancyDefault);
+    for (int m = 0; m < 4; ++m)
+        if (p.sb[m]) {
+            allow_smem(p.sb[m], smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&p.sb_bps[m], p.sb[m], LS * (N / E), smem,
+                                                                  cudaOccupancyDefault);
+        }
+    cudaGetLastError();
     return p;
 }
 
@@ -86,11 +117,21 @@ void add_x_variant(PlanEntry<T>& p) {
     v.k[XM_MID] = xpass3_kernel<T, XM_MID, N, E, R0, R1, R2, NW, NBUF, MINB>;
     v.k[XM_END] = xpass3_kernel<T, XM_END, N, E, R0, R1, R2, NW, NBUF, MINB>;
     const size_t psi = (size_t)LPC * N * sizeof(cx<T>);
+    if constexpr (sizeof(T) == 4) {  // batched forms for the complex64 batch path
+        v.kb[XM_START] = xbatch3_kernel<T, XM_START, N, E, R0, R1, R2, NW, NBUF, MINB>;
+        v.kb[XM_MID] = xbatch3_kernel<T, XM_MID, N, E, R0, R1, R2, NW, NBUF, MINB>;
+        v.kb[XM_END] = xbatch3_kernel<T, XM_END, N, E, R0, R1, R2, NW, NBUF, MINB>;
+    }
     for (int m : {XM_FWD, XM_START, XM_MID, XM_END}) {
         v.smem[m] = NBUF * (m != XM_FWD ? 2 * psi : psi) + NBUF * sizeof(uint64_t);
         allow_smem(v.k[m], (int)v.smem[m]);
         cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bps[m], v.k[m], NW * 32, v.smem[m],
                                                               cudaOccupancyDefault);
+        if (v.kb[m]) {
+            allow_smem(v.kb[m], (int)v.smem[m]);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bbps[m], v.kb[m], NW * 32, v.smem[m],
+                                                                  cudaOccupancyDefault);
+        }
     }
     cudaGetLastError();
     p.xv.push_back(v);
@@ -105,11 +146,21 @@ void add_s_variant(PlanEntry<T>& p) {
     v.k[SM_FWD] = spass3_kernel<T, SM_FWD, N, E, R0, R1, R2, LS, NBUF, MINB>;
     v.k[SM_INV] = spass3_kernel<T, SM_INV, N, E, R0, R1, R2, LS, NBUF, MINB>;
     v.k[SM_FUSED] = spass3_kernel<T, SM_FUSED, N, E, R0, R1, R2, LS, NBUF, MINB>;
+    if constexpr (sizeof(T) == 4) {
+        v.kb[SM_FWD] = sbatch3_kernel<T, SM_FWD, N, E, R0, R1, R2, LS, NBUF, MINB>;
+        v.kb[SM_INV] = sbatch3_kernel<T, SM_INV, N, E, R0, R1, R2, LS, NBUF, MINB>;
+        v.kb[SM_FUSED] = sbatch3_kernel<T, SM_FUSED, N, E, R0, R1, R2, LS, NBUF, MINB>;
+    }
     v.smem = NBUF * (size_t)N * LS * sizeof(cx<T>) + NBUF * sizeof(uint64_t);
     for (int m : {SM_FWD, SM_INV, SM_FUSED}) {
         allow_smem(v.k[m], (int)v.smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bps[m], v.k[m], LS * TL, v.smem,
                                                               cudaOccupancyDefault);
+        if (v.kb[m]) {
+            allow_smem(v.kb[m], (int)v.smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bbps[m], v.kb[m], LS * TL, v.smem,
+                                                                  cudaOccupancyDefault);
+        }
     }
     cudaGetLastError();
     p.sv.push_back(v);

@@ -1,12 +1,25 @@
-// Compiled plans with radix-3/5 stages: 48, 96, 160 (160: complex64 only).
+// Compiled plans with radix-3/5 factors: 48 = 4x4x3, 96 = 6x4x4, 160 = 10x4x4
+// (radix 6 and 10 are prime-factor butterflies), with pipelined complex64 variants.
 #include "ses_plans.cuh"
 
 namespace sesk {
 void register_plans_mixed(std::vector<PlanEntry<float>>& f, std::vector<PlanEntry<double>>& d) {
     f.push_back(make_plan_entry<float, 48, 12, 4, 4, 3, 32>());
+    add_x_variant<float, 48, 12, 4, 4, 3, 4, 2, 3>(f.back());
+    add_s_variant<float, 48, 12, 4, 4, 3, 48, 2, 3>(f.back());
+    add_s_variant<float, 48, 12, 4, 4, 3, 16, 2, 8>(f.back());
     d.push_back(make_plan_entry<double, 48, 12, 4, 4, 3, 16>());
-    f.push_back(make_plan_entry<float, 96, 24, 8, 4, 3, 32>());
-    d.push_back(make_plan_entry<double, 96, 24, 8, 4, 3, 16>());
-    f.push_back(make_plan_entry<float, 160, 40, 8, 4, 5, 32>());
+    f.push_back(make_plan_entry<float, 96, 12, 6, 4, 4, 32>());
+    add_x_variant<float, 96, 12, 6, 4, 4, 4, 2, 3>(f.back());
+    add_x_variant<float, 96, 12, 6, 4, 4, 2, 2, 6>(f.back());
+    add_s_variant<float, 96, 12, 6, 4, 4, 32, 2, 2>(f.back());
+    add_s_variant<float, 96, 12, 6, 4, 4, 16, 2, 4>(f.back());
+    d.push_back(make_plan_entry<double, 96, 12, 6, 4, 4, 16>());
+    f.push_back(make_plan_entry<float, 160, 20, 10, 4, 4, 32>());
+    add_x_variant<float, 160, 20, 10, 4, 4, 4, 2, 2>(f.back());
+    add_x_variant<float, 160, 20, 10, 4, 4, 2, 2, 4>(f.back());
+    add_s_variant<float, 160, 20, 10, 4, 4, 32, 2, 2>(f.back());
+    add_s_variant<float, 160, 20, 10, 4, 4, 16, 2, 4>(f.back());
+    d.push_back(make_plan_entry<double, 160, 20, 10, 4, 4, 16>());
 }
 }  // namespace sesk

@@ -185,3 +185,35 @@ def config_c3(n: int = 512) -> Workload:
                     gaussian(g, (-20.0, 0.0, 0.0), (3.0, 3.0, 3.0), (3.0, 0.0, 0.0)), 0.002, 500,
                     mask=mask_profiles(g, 0.08), observe_every=50, x_range=(1.0, math.inf),
                     meta={"seed": SEED_BASE + 2, "barrier_height": v0})
+
+
+C4_SIZES = (32, 48, 64, 96, 128, 160)
+
+
+def config_c4_specs(count: int = 256, sizes=C4_SIZES, seed: int = SEED_BASE + 3) -> list[dict]:
+    """Batched tunnelling sweep: `count` independent 3D instances, n uniform over
+    `sizes`, box side 20 n/32 centred on 0 (spacing 0.625 at every n), barrier of
+    thickness 2 at x = 0 with height U[0.5, 4], packet sigma U[1, 2.5] (isotropic)
+    at x = -L/4 with k0 = (U[1, 4], 0, 0), cos^(1/8) absorber on the outer 8%,
+    complex64 with FP64-built tables, dt 0.005, 1000 steps.  Drawn in this order
+    per instance: n, height, k0, sigma."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(sizes[int(rng.integers(0, len(sizes)))])
+        v0 = float(rng.uniform(0.5, 4.0))
+        k0 = float(rng.uniform(1.0, 4.0))
+        sigma = float(rng.uniform(1.0, 2.5))
+        out.append({"index": i, "n": n, "side": 20.0 * n / 32.0, "barrier": v0, "k0": k0,
+                    "sigma": sigma, "dt": 0.005, "steps": 1000, "mask_frac": 0.08})
+    return out
+
+
+def build_c4_instance(spec: dict) -> Workload:
+    half = 0.5 * spec["side"]
+    g = cube_grid(-half, half, spec["n"])
+    s = spec["sigma"]
+    psi0 = gaussian(g, (-0.5 * half, 0.0, 0.0), (s, s, s), (spec["k0"], 0.0, 0.0))
+    return Workload(f"c4_tunnel_{spec['n']}_{spec['index']}", g, barrier(g, spec["barrier"], -1.0, 1.0),
+                    psi0, spec["dt"], spec["steps"], mask=mask_profiles(g, spec["mask_frac"]),
+                    observe_every=100, x_range=(1.0, math.inf), meta=dict(spec))

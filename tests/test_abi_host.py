@@ -203,7 +203,7 @@ def test_plans_stay_in_bounds(dims, es):
 # fused passes -- modelled exactly and compared with numpy's FFT.
 
 COMPILED_PLANS = [(16, 16, (16,)), (32, 8, (8, 4)), (48, 12, (4, 4, 3)), (64, 8, (8, 8)),
-                  (96, 24, (8, 4, 3)), (128, 16, (16, 8)), (160, 40, (8, 4, 5)), (256, 16, (16, 16)),
+                  (96, 12, (6, 4, 4)), (128, 16, (16, 8)), (160, 20, (10, 4, 4)), (256, 16, (16, 16)),
                   (512, 16, (8, 8, 8)), (1024, 32, (16, 8, 8))]
 
 
@@ -275,3 +275,30 @@ def test_compiled_plan_index_model(plan):
     # the reversed plan consumes the forward plan's register layout directly
     z = model_fft(y, N, E, tuple(reversed(rads)), tab, fwd_entries)
     assert np.allclose(z, np.fft.fft(np.fft.fft(x)), rtol=0, atol=1e-10 * np.abs(z).max())
+
+
+def test_batch_arguments_without_device():
+    from shoeridingerequationsolver_b200 import _abi
+    assert _abi.lib.ses_batch_step(None, 1, 0) == _abi.SES_EINVAL
+    assert _abi.lib.ses_batch_add(None, None) == _abi.SES_EINVAL
+    assert _abi.lib.ses_batch_observe(None, 0.0, 1.0, None, 0) == _abi.SES_EINVAL
+    b = C.c_void_p()
+    st = _abi.lib.ses_batch_create(C.byref(b))
+    if st == _abi.SES_OK:                      # a device is visible
+        assert _abi.lib.ses_batch_step(b, -1, 0) == _abi.SES_EINVAL
+        assert _abi.lib.ses_batch_step(b, 5, 0) == _abi.SES_OK    # empty batch: nothing to do
+        assert _abi.lib.ses_batch_destroy(b) == _abi.SES_OK
+    else:
+        assert st == _abi.SES_EDEVICE and not b.value
+
+
+def test_c4_specs_are_seeded_and_cover_every_size():
+    from shoeridingerequationsolver_b200 import scenes
+    a, b = scenes.config_c4_specs(), scenes.config_c4_specs()
+    assert a == b and len(a) == 256
+    assert {s["n"] for s in a} == set(scenes.C4_SIZES)
+    for s in a:
+        assert 0.5 <= s["barrier"] <= 4.0 and 1.0 <= s["k0"] <= 4.0 and 1.0 <= s["sigma"] <= 2.5
+        assert abs(s["side"] / s["n"] - 0.625) < 1e-15
+    w = scenes.build_c4_instance(a[0])
+    assert w.grid.dims == (a[0]["n"],) * 3 and w.psi0.size == a[0]["n"] ** 3

@@ -1,0 +1,139 @@
+"""Batched propagation (ses_batch_*): many fields of mixed shapes advanced by one
+launch per axis pass and shape class.
+
+Every member must end where the same handle stepped alone ends: the batched
+kernels run the same line-FFT bodies over per-instance arguments, so a member's
+arithmetic does not depend on who else is in the batch.  They are separate
+kernels from the single-handle ones, so the compiler may contract a different
+multiply-add here and there: results agree to rounding (relative L2 below
+TOL), not bit for bit.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+from shoeridingerequationsolver_b200 import scenes
+
+TOL = {"c128": 1e-14, "c64": 5e-7}
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def make_member(ses, shape, box, prec, seed, dt=0.01, absorber=True):
+    rng = np.random.default_rng(seed)
+    axes = [ses.Grid1D(-box[a], box[a], shape[a]) for a in range(3)]
+    g = ses.Grid3D(*axes)
+    V = scenes.harmonic(g, float(rng.uniform(0.5, 1.5)), tuple(rng.uniform(-0.5, 0.5, 3)))
+    c = [float(rng.uniform(-0.3, 0.3)) * box[a] if shape[a] > 1 else 0.0 for a in range(3)]
+    psi = scenes.gaussian(g, c, [max(0.12 * box[a], 0.3) for a in range(3)],
+                          [float(rng.uniform(-1, 1)) if shape[a] > 1 else 0.0 for a in range(3)])
+    op = ses.SplitOperator3D(g, V, dt, precision=prec)
+    op.upload_state(psi)
+    if absorber:
+        op.set_absorber_separable(*scenes.mask_profiles(g, 0.1))
+    return op, psi
+
+
+SHAPES = [(16, 16, 16), (32, 32, 32), (48, 48, 48), (32, 16, 48), (96, 96, 1), (128, 1, 1),
+          (64, 64, 64)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+@pytest.mark.parametrize("nsteps", [1, 3, 11])
+def test_batch_members_match_alone(ses, prec, nsteps):
+    box = (8.0, 7.0, 6.0)
+    members, alone = [], []
+    for i, shape in enumerate(SHAPES + SHAPES[:3]):   # repeated shapes share a class
+        op, psi = make_member(ses, shape, box, prec, seed=100 + i)
+        ref, _ = make_member(ses, shape, box, prec, seed=100 + i)
+        members.append(op)
+        alone.append(ref)
+    with ses.Batch(members) as b:
+        assert b.counts() == (len(members), len(SHAPES))
+        b.step(nsteps, absorb=True)
+        b.sync()
+        for op, ref, shape in zip(members, alone, SHAPES + SHAPES[:3]):
+            ref.advance(nsteps, absorb=True)
+            got, want = op.readback(), ref.readback()
+            assert np.all(np.isfinite(got))
+            assert rel(got, want) <= TOL[prec], shape
+    for op in members + alone:
+        op.close()
+
+
+@pytest.mark.gpu
+def test_batch_member_vs_oracle_mixed_radix(ses, oracle):
+    """A 48^3 and a 96x96 member of a batch against the FP64 oracle step."""
+    box = (6.0, 6.0, 6.0)
+    ops = []
+    for i, shape in enumerate([(48, 48, 48), (96, 96, 1)]):
+        op, psi = make_member(ses, shape, box, "c128", seed=7 + i, absorber=False)
+        rng = np.random.default_rng(7 + i)   # the potential make_member drew
+        V = scenes.harmonic(op.grid, float(rng.uniform(0.5, 1.5)), tuple(rng.uniform(-0.5, 0.5, 3)))
+        ops.append((op, psi, V))
+    with ses.Batch([o for o, _, _ in ops]) as b:
+        b.step(5)
+        b.sync()
+        for op, psi, V in ops:
+            g = op.grid
+            want = oracle.step3d(g.box, g.dims, V, 0.01, psi, 5)
+            assert rel(op.readback(), want) <= 5e-12, g.dims
+    for op, _, _ in ops:
+        op.close()
+
+
+@pytest.mark.gpu
+def test_batch_membership_changes(ses):
+    """Remove, re-add and destroy members between steps; the rest keep stepping
+    exactly as alone; observe returns one record per member in add order."""
+    box = (8.0, 8.0, 8.0)
+    ops = [make_member(ses, s, box, "c64", seed=40 + i)[0] for i, s in enumerate(SHAPES[:4])]
+    refs = [make_member(ses, s, box, "c64", seed=40 + i)[0] for i, s in enumerate(SHAPES[:4])]
+    b = ses.Batch(ops)
+    b.step(4, absorb=True)
+    for r in refs:
+        r.advance(4, absorb=True)
+    b.remove(ops[1])
+    with pytest.raises(Exception):
+        b.remove(ops[1])                       # not a member any more
+    ops[1].advance(2, absorb=True)             # steps alone on its own stream again
+    refs[1].advance(2, absorb=True)
+    ops[2].close()                             # destroying a member removes it first
+    b.step(3, absorb=True)
+    for i in (0, 3):
+        refs[i].advance(3, absorb=True)
+    obs = b.observe()
+    assert len(obs) == 2
+    for rec, i in zip(obs, (0, 3)):
+        assert math.isclose(rec["norm"], refs[i].observe()["norm"], rel_tol=1e-6)
+        assert rel(ops[i].readback(), refs[i].readback()) <= TOL["c64"]
+    assert rel(ops[1].readback(), refs[1].readback()) <= TOL["c64"]
+    b.add(ops[1])
+    with pytest.raises(Exception):
+        b.add(ops[1])                          # already a member
+    b.close()
+    for i in (0, 1, 3):
+        ops[i].close()
+    for r in refs:
+        r.close()
+
+
+@pytest.mark.gpu
+def test_batch_profile_reports_every_class(ses):
+    box = (8.0, 8.0, 8.0)
+    ops = [make_member(ses, s, box, "c64", seed=60 + i)[0] for i, s in enumerate(SHAPES[:3])]
+    with ses.Batch(ops) as b:
+        prof = b.profile(4, absorb=True)
+        assert len(prof) == 3
+        for p in prof:
+            assert p["step"] > 0 and p["x_mid"] > 0
+        for op in ops:
+            o = op.observe()
+            assert 0.5 < o["norm"] <= 1.0 + 1e-6
+    for op in ops:
+        op.close()
