@@ -241,6 +241,68 @@ SES_API ses_status ses_batch_autotune(ses_batch b, int flags);
 /* One line per class: shape, precision, members and the kernel of each pass. */
 SES_API ses_status ses_batch_info(ses_batch b, char* buf, size_t len);
 
+/* ---- serving: continuous batching of solve requests ----
+ * No direct counterpart in the reference, whose directors run one scene per
+ * Engine (solver/src/vk_engine.ixx:597-698, scenario/src/base_director.ixx)
+ * and whose sweeps loop over instances on the CPU.  A server owns one batch
+ * and a worker thread.  Requests are admitted first come, first served while
+ * their estimated device bytes fit the budget; admitted fields and tables
+ * stay resident in HBM.  All running requests advance together in rounds that
+ * end at the earliest observation point or completion of any of them; new
+ * requests join and finished ones leave between rounds.  Observables
+ * (ses_gpu_observe) are recorded every observe_every steps and at
+ * completion; latency is submission to completion.  Every call is
+ * thread-safe. */
+typedef struct ses_server_s* ses_server;
+
+typedef struct ses_request {
+    ses_grid_desc grid;
+    ses_precision prec;
+    double dt, mass;            /* mass <= 0 means 1 */
+    const double* V;            /* nx*ny*nz doubles, copied at submit */
+    const double* psi0;         /* nx*ny*nz interleaved complex128, copied at submit */
+    const double* mask_x;       /* separable absorber profiles (nx, ny, nz doubles), */
+    const double* mask_y;       /* applied after every step; all three or none */
+    const double* mask_z;
+    int32_t nsteps;             /* >= 1 */
+    int32_t observe_every;      /* 0: observe at completion only */
+    double xlo, xhi;            /* interval of ses_observables.p_range */
+} ses_request;
+
+typedef struct ses_record {
+    int64_t id;
+    int32_t step;               /* steps completed when observed */
+    int32_t final_record;       /* 1 on the record taken at completion */
+    double t_ms;                /* since submission */
+    ses_observables obs;
+} ses_record;
+
+enum { SES_REQ_QUEUED = 0, SES_REQ_RUNNING = 1, SES_REQ_DONE = 2, SES_REQ_CANCELLED = 3, SES_REQ_FAILED = 4 };
+
+typedef struct ses_serve_stats_t {
+    int64_t submitted, admitted, completed, cancelled, failed, queued, running, rounds;
+    size_t bytes_in_use, budget;
+    double gridpt_steps;        /* grid points x steps advanced by all rounds */
+    double busy_ms;             /* wall time spent in rounds */
+    double wall_ms;             /* since open */
+    double latency_p50_ms, latency_p99_ms;  /* over completed requests */
+} ses_serve_stats_t;
+
+/* max_round_steps: longest round (0: 100). */
+SES_API ses_status ses_serve_open(size_t budget_bytes, int max_round_steps, ses_server* out);
+/* Copies the request's arrays; SES_ENOMEM if it can never fit the budget. */
+SES_API ses_status ses_serve_submit(ses_server s, const ses_request* r, int64_t* id);
+/* Moves up to cap pending records of request id into recs; *state = SES_REQ_*. */
+SES_API ses_status ses_serve_poll(ses_server s, int64_t id, ses_record* recs, int cap, int* n, int* state);
+/* After SES_REQ_DONE: the final psi (interleaved complex128, once) and the latency. */
+SES_API ses_status ses_serve_result(ses_server s, int64_t id, double* psi_out, double* latency_ms);
+SES_API ses_status ses_serve_cancel(ses_server s, int64_t id);
+/* Waits (bounded) until every submitted request has finished. */
+SES_API ses_status ses_serve_wait_idle(ses_server s, int timeout_ms);
+SES_API ses_status ses_serve_stats(ses_server s, ses_serve_stats_t* out);
+/* Cancels whatever is still queued or running, joins the worker, frees everything. */
+SES_API ses_status ses_serve_close(ses_server s);
+
 /* ---- fft surface on host arrays (core/src/fft.ixx:75-188) ----
  * fft(std::vector<cd>&) / ifft(...) and fft(Field3D&) / ifft(Field3D&):
  * n[3] = (nx, ny, nz), data = interleaved complex128, transformed in place

@@ -26,6 +26,8 @@ EXPORTS = [
     "ses_batch_create", "ses_batch_destroy", "ses_batch_add", "ses_batch_remove", "ses_batch_step",
     "ses_batch_observe", "ses_batch_sync", "ses_batch_set_stream", "ses_batch_members",
     "ses_batch_profile", "ses_batch_autotune", "ses_batch_info",
+    "ses_serve_open", "ses_serve_submit", "ses_serve_poll", "ses_serve_result", "ses_serve_cancel",
+    "ses_serve_wait_idle", "ses_serve_stats", "ses_serve_close",
 ]
 
 
@@ -50,6 +52,32 @@ class Observables(C.Structure):
             "mean_pos": list(self.mean_pos), "sigma_pos": list(self.sigma_pos),
             "mean_mom": list(self.mean_mom),
         }
+
+
+class Request(C.Structure):
+    _fields_ = [("grid", GridDesc), ("prec", C.c_int), ("dt", C.c_double), ("mass", C.c_double),
+                ("V", C.c_void_p), ("psi0", C.c_void_p), ("mask_x", C.c_void_p), ("mask_y", C.c_void_p),
+                ("mask_z", C.c_void_p), ("nsteps", C.c_int32), ("observe_every", C.c_int32),
+                ("xlo", C.c_double), ("xhi", C.c_double)]
+
+
+class Record(C.Structure):
+    _fields_ = [("id", C.c_int64), ("step", C.c_int32), ("final_record", C.c_int32), ("t_ms", C.c_double),
+                ("obs", Observables)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "admitted", "completed", "cancelled", "failed",
+                                          "queued", "running", "rounds")] + \
+               [("bytes_in_use", C.c_size_t), ("budget", C.c_size_t), ("gridpt_steps", C.c_double),
+                ("busy_ms", C.c_double), ("wall_ms", C.c_double), ("latency_p50_ms", C.c_double),
+                ("latency_p99_ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_CANCELLED, REQ_FAILED = range(5)
 
 
 class SesError(RuntimeError):
@@ -103,6 +131,15 @@ def _load() -> C.CDLL:
         "ses_batch_profile": ([vp, C.c_int, C.c_int, dp, C.c_int], st),
         "ses_batch_autotune": ([vp, C.c_int], st),
         "ses_batch_info": ([vp, C.c_char_p, C.c_size_t], st),
+        "ses_serve_open": ([C.c_size_t, C.c_int, C.POINTER(vp)], st),
+        "ses_serve_submit": ([vp, C.POINTER(Request), C.POINTER(C.c_int64)], st),
+        "ses_serve_poll": ([vp, C.c_int64, C.POINTER(Record), C.c_int, C.POINTER(C.c_int),
+                            C.POINTER(C.c_int)], st),
+        "ses_serve_result": ([vp, C.c_int64, vp, dp], st),
+        "ses_serve_cancel": ([vp, C.c_int64], st),
+        "ses_serve_wait_idle": ([vp, C.c_int], st),
+        "ses_serve_stats": ([vp, C.POINTER(ServeStats)], st),
+        "ses_serve_close": ([vp], st),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

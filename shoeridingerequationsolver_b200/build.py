@@ -18,7 +18,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libses_b200.so"
 SOURCES = ["ses_gpu.cu", "ses_plans_small.cu", "ses_plans_mixed.cu", "ses_plans_256.cu",
-           "ses_plans_large.cu", "ses_noalloc.cu"]
+           "ses_plans_large.cu", "ses_noalloc.cu", "ses_serve.cpp"]
 HEADERS = ["ses_fft.cuh", "ses_pass.cuh", "ses_pass2.cuh", "ses_pass3.cuh", "ses_tma.cuh", "ses_plans.cuh",
            "ses_aux.cuh"]
 

@@ -42,10 +42,6 @@ struct Tables {
 };
 
 // complex64 phase multiplies in FP32 on the delta form: psi + psi*d, d = factor - 1.
-// (1 + d)^2 - 1 = 2d + d^2 for the full potential kick between steps.
-__device__ __forceinline__ cx<float> delta_full(cx<float> d) {
-    return mk<float>(fmaf(d.x, d.x, fmaf(-d.y, d.y, 2.0f * d.x)), fmaf(2.0f * d.x, d.y, 2.0f * d.y));
-}
 __device__ __forceinline__ cx<float> add_mul(cx<float> p, cx<float> d) {  // p + p*d
     return mk<float>(fmaf(p.x, d.x, fmaf(-p.y, d.y, p.x)), fmaf(p.x, d.y, fmaf(p.y, d.x, p.y)));
 }
@@ -95,57 +91,36 @@ __device__ __forceinline__ cx<T> apply_diag_tv(cx<T> v, int kind, cx<T> tab, int
 template <typename T>
 __device__ __forceinline__ cx<T> apply_diag(cx<T> v, int kind, int use_mask, long long f, int i, int j,
                                             int k, const Tables& tb) {
-    if constexpr (sizeof(T) == 4) {
-        const cx<T> tab = kind != DG_NONE ? reinterpret_cast<const cx<T>*>(tb.vtab)[f] : v;
-        return apply_diag_tv(v, kind, tab, use_mask, use_mask ? maskval<T>(tb, f, i, j, k) : 1.0);
-    }
-    cx<double> p = widen(v);
-    if (kind != DG_NONE) {
-        if constexpr (sizeof(T) == 8) {
-            const cx<double> h = reinterpret_cast<const cx<double>*>(tb.vtab)[f];
-            p = p * (kind == DG_FULL ? h * h : h);
-        } else {
-            cx<double> d = widen(reinterpret_cast<const cx<float>*>(tb.vtab)[f]);
-            if (kind == DG_FULL)  // (1 + d)^2 - 1 = 2d + d^2
-                d = mk<double>(2.0 * d.x + (d.x * d.x - d.y * d.y), 2.0 * d.y + 2.0 * d.x * d.y);
-            p = p + p * d;
-        }
-    }
-    if (use_mask) {
-        const double m = maskval<T>(tb, f, i, j, k);
-        p = mk<double>(p.x * m, p.y * m);
-    }
-    return narrow<T>(p);
+    const cx<T> tab = kind != DG_NONE ? reinterpret_cast<const cx<T>*>(tb.vtab)[f] : v;
+    return apply_diag_tv(v, kind, tab, use_mask, use_mask ? maskval<T>(tb, f, i, j, k) : 1.0);
 }
 
 // Same as apply_diag with the potential-table entry and mask value supplied
-// by the caller (pipelined passes stage the table in shared memory).  The
-// complex64 path multiplies in FP32 on the delta form.
+// by the caller (pipelined passes stage the table in shared memory).
+//   DG_HALF: psi * h (* m)            h = cis(-V dt/2)
+//   DG_FULL: (psi * h (* m)) * h      the kick between two steps, applied as the
+//            half kick that ends one step (with the mask) followed by the half
+//            kick that starts the next, in exactly that arithmetic -- so a run
+//            of steps split into two calls gives the same bits as one call.
+// The complex64 path multiplies in FP32 on the delta form psi + psi*d, d = h - 1.
 template <typename T>
 __device__ __forceinline__ cx<T> apply_diag_tv(cx<T> v, int kind, cx<T> tab, int use_mask, double m) {
     if constexpr (sizeof(T) == 4) {
         cx<float> p = v;
-        if (kind != DG_NONE) p = add_mul(p, kind == DG_FULL ? delta_full(tab) : tab);
+        if (kind != DG_NONE) p = add_mul(p, tab);
         if (use_mask) {
             const float mf = (float)m;
             p = mk<float>(p.x * mf, p.y * mf);
         }
+        if (kind == DG_FULL) p = add_mul(p, tab);
+        return p;
+    } else {
+        cx<double> p = v;
+        if (kind != DG_NONE) p = p * tab;
+        if (use_mask) p = mk<double>(p.x * m, p.y * m);
+        if (kind == DG_FULL) p = p * tab;
         return p;
     }
-    cx<double> p = widen(v);
-    if (kind != DG_NONE) {
-        if constexpr (sizeof(T) == 8) {
-            const cx<double> h = widen(tab);
-            p = p * (kind == DG_FULL ? h * h : h);
-        } else {
-            cx<double> d = widen(tab);
-            if (kind == DG_FULL)  // (1 + d)^2 - 1 = 2d + d^2
-                d = mk<double>(2.0 * d.x + (d.x * d.x - d.y * d.y), 2.0 * d.y + 2.0 * d.x * d.y);
-            p = p + p * d;
-        }
-    }
-    if (use_mask) p = mk<double>(p.x * m, p.y * m);
-    return narrow<T>(p);
 }
 
 __device__ __forceinline__ double mask_at(const Tables& tb, long long f, int i, int j, int k) {

@@ -153,7 +153,12 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
     constexpr int PITCH = XS::PITCH;
     constexpr int NW = XS::NW;
     using S = PlanShape<R0, R1, R2>;
-    constexpr int RF = R0, RL = S::last;
+    // The batch-start pass runs its forward FFT in the reversed radix order, the
+    // order of the second FFT of the between-steps pass, so that a batch end
+    // followed by a batch start computes what one between-steps pass computes.
+    constexpr bool kRev = MODE == XM_START;
+    constexpr int RF = kRev ? S::last : R0;  // radix of the first FFT's first stage
+    constexpr int RL = kRev ? R0 : S::last;  // radix of its last stage (output layout)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int lw = lane / TL, q = lane % TL;
     const long long m = (blk * NW + warp) * LPW + lw;
@@ -181,7 +186,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
             v[b * RF + r] = kConjIn ? cconj(e) : e;
         }
 
-    rfft_plan<T, N, E, R0, R1, R2, false>(v, q, a.stw, a.stwl, x);
+    rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, a.stw, a.stwl, x);
     // v[b*RL + r] now at position q + TL b + r N/RL
 
     if constexpr (MODE == XM_REDUCE) {

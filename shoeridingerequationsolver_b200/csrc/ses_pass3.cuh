@@ -219,7 +219,10 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
     constexpr uint32_t PSI_BYTES = (uint32_t)(LPC * N * sizeof(cx<T>));
     constexpr uint32_t BUF_BYTES = kTab ? 2 * PSI_BYTES : PSI_BYTES;
     using S = PlanShape<R0, R1, R2>;
-    constexpr int RF = R0, RL = S::last;
+    // batch start: reversed radix order, as the second FFT of the between-steps pass
+    constexpr bool kRev = MODE == XM_START;
+    constexpr int RF = kRev ? S::last : R0;
+    constexpr int RL = kRev ? R0 : S::last;
     extern __shared__ __align__(1024) unsigned char smraw3[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smraw3 + (size_t)NBUF * BUF_BYTES);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -295,7 +298,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                 v[b * RF + r] = kConjIn ? cconj(e) : e;
             }
         __syncwarp();  // the line is reused for exchanges: all stage-0 reads first
-        rfft_plan<T, N, E, R0, R1, R2, false>(v, q, a.stw, a.stwl, x);
+        rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, a.stw, a.stwl, x);
 
         if constexpr (MODE == XM_FWD || MODE == XM_START || MODE == XM_END) {
             if (valid) {

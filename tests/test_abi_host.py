@@ -302,3 +302,19 @@ def test_c4_specs_are_seeded_and_cover_every_size():
         assert abs(s["side"] / s["n"] - 0.625) < 1e-15
     w = scenes.build_c4_instance(a[0])
     assert w.grid.dims == (a[0]["n"],) * 3 and w.psi0.size == a[0]["n"] ** 3
+
+
+def test_serve_arguments_without_device():
+    from shoeridingerequationsolver_b200 import _abi
+    rid = C.c_int64()
+    assert _abi.lib.ses_serve_submit(None, None, C.byref(rid)) == _abi.SES_EINVAL
+    assert _abi.lib.ses_serve_close(None) == _abi.SES_EINVAL
+    s = C.c_void_p()
+    assert _abi.lib.ses_serve_open(0, 0, C.byref(s)) == _abi.SES_EINVAL
+    st = _abi.lib.ses_serve_open(1 << 30, 0, C.byref(s))
+    if st == _abi.SES_OK:                      # a device is visible
+        r = _abi.Request()
+        assert _abi.lib.ses_serve_submit(s, C.byref(r), C.byref(rid)) == _abi.SES_EINVAL
+        assert _abi.lib.ses_serve_close(s) == _abi.SES_OK
+    else:
+        assert st == _abi.SES_EDEVICE
