@@ -78,6 +78,29 @@ __global__ void build_twiddles(int n, cx<T>* tw) {
     }
 }
 
+// Long 1D line of N = N1 N2 points in the four-step layout: the element stored
+// at (k1, k2) after the forward transform (flat k1 + N1 k2) is frequency
+// k = k2 + N2 k1; its kinetic delta is cis(-k_phys^2 dt/(2m)) - 1 with k_phys the
+// line's fftfreq wavenumber kv[k].  The twiddle of element (n1, k2) is
+// W_N^{n1 k2} = e^{-2 pi i (n1 k2 mod N)/N}, in FP64 (complex64: hi + lo parts).
+template <typename T>
+__global__ void build_long_tables(const double* __restrict__ kv, int n1, int n2, double dt, double mass,
+                                  cx<T>* kfull, cx<T>* tw_hi, cx<T>* tw_lo) {
+    const long long N = (long long)n1 * n2;
+    for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < N;
+         f += (long long)gridDim.x * blockDim.x) {
+        const long long a = f % n1, b = f / n1;  // (k1, k2) for kfull, (n1, k2) for the twiddle
+        const double k = kv[b + (long long)n2 * a];
+        const cx<double> d = cis_minus_one(theta_k(__dmul_rn(k, k), mass, dt));
+        kfull[f] = mk<T>((T)d.x, (T)d.y);
+        const long long t = (a * b) % N;
+        double sn, cs;
+        sincospi(-2.0 * (double)t / (double)N, &sn, &cs);
+        tw_hi[f] = mk<T>((T)cs, (T)sn);
+        if (tw_lo) tw_lo[f] = mk<T>((T)(cs - (double)(T)cs), (T)(sn - (double)(T)sn));
+    }
+}
+
 // Full-N reference tables (propagator-tables surface).
 __global__ void build_full_tables(const double* __restrict__ V, const double* __restrict__ kvx,
                                   const double* __restrict__ kvy, const double* __restrict__ kvz,

@@ -43,6 +43,19 @@ template <typename T>
 __device__ __forceinline__ cx<T> scale(cx<T> a, T s) {
     return mk<T>(a.x * s, a.y * s);
 }
+// a * s for an FP64 scale s such as 1/N, which is not a power of two for
+// radix-3/5 sizes: complex64 carries s as hi + lo, so that the scale applied
+// every step has no systematic rounding (a plain FP32 1/N is off by up to 6e-8,
+// which would move the norm by ~1e-7 every step).
+template <typename T>
+__device__ __forceinline__ cx<T> scale_d(cx<T> a, double s) {
+    if constexpr (sizeof(T) == 4) {
+        const float hi = (float)s, lo = (float)(s - (double)hi);
+        return mk<float>(fmaf(a.x, hi, a.x * lo), fmaf(a.y, hi, a.y * lo));
+    } else {
+        return mk<double>(a.x * s, a.y * s);
+    }
+}
 // a * (-i)
 template <typename T>
 __device__ __forceinline__ cx<T> mul_mi(cx<T> a) {

@@ -261,9 +261,18 @@ struct ses_solver {
     int xsel = 0;                  // pipelined contiguous-pass variant (-1: register path)
     int ssel[3] = {0, 0, 0};       // pipelined strided-pass variant per axis (-1: register path)
     ses_batch_s* batch = nullptr;  // batch this handle belongs to (its stream is the batch's)
+    // long 1D line (nx > 4096, ny = nz = 1) stored as n[0] x n[1] = N1 x N2 and
+    // transformed in four steps; box[0..1] and N keep the physical line
+    bool long1d = false;
+    void* kfull = nullptr;   // kinetic delta per stored k-space element
+    void* tw4 = nullptr;     // W_N^{n1 k2} per element (complex64: hi part)
+    void* tw4l = nullptr;    // complex64: lo part
 };
 
 namespace {
+
+// Physical axis length (the layout axes of a long line differ from it).
+int phys_n(const ses_solver* h, int a) { return h->long1d ? (a == 0 ? (int)h->N : 1) : h->n[a]; }
 
 ses_status dalloc(ses_solver* h, void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
@@ -288,7 +297,7 @@ void release(ses_solver* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
-    void* ptrs[] = {h->psi, h->scratch, h->vtab, h->V, h->maskfull, h->partials, h->dsums};
+    void* ptrs[] = {h->psi, h->scratch, h->vtab, h->V, h->maskfull, h->partials, h->dsums, h->kfull, h->tw4, h->tw4l};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int a = 0; a < 3; ++a) {
@@ -386,6 +395,10 @@ PassArgs<T> make_args(const ses_solver* h, int axis, const void* src, void* dst)
     tb.maskfull = h->maskfull;
     tb.inv_mass = 1.0 / h->mass;
     tb.kscale = 1.0 / (double)h->N;
+    tb.kfull = h->kfull;
+    tb.tw4 = h->tw4;
+    tb.tw4l = h->tw4l;
+    tb.long_n2 = h->long1d ? h->n[1] : 0;
     a.partials = h->partials;
     return a;
 }
@@ -494,6 +507,27 @@ ses_status pass_s(const ses_solver* h, int axis, const void* src, void* dst, int
     return launch<T>(h, axis, mode, a, s);
 }
 
+// Strided pass of a long line (SM_TW_*), with its potential/mask program.
+template <typename T>
+ses_status pass_tw(const ses_solver* h, const void* src, void* dst, int mode, const XProg& p, cudaStream_t s) {
+    PassArgs<T> a = make_args<T>(h, 1, src, dst);
+    a.d_load = p.d_load;
+    a.d_mid = p.d_mid;
+    a.d_store = p.d_store;
+    a.m_load = p.m_load;
+    a.m_mid = p.m_mid;
+    a.m_store = p.m_store;
+    return launch<T>(h, 1, mode, a, s);
+}
+
+// x pass of a long line: fwd, kinetic (per-element table), inv.
+template <typename T>
+ses_status pass_long_x(const ses_solver* h, cudaStream_t s) {
+    XProg p;
+    p.mode = XM_1D;
+    return pass_x<T>(h, h->psi, h->psi, p, s);
+}
+
 template <typename T>
 void set_attrs_prec() {
     for (int m = XM_FWD; m <= XM_REDUCE; ++m) set_smem_attr(xkernel<T>(m));
@@ -525,6 +559,12 @@ ses_status mid_axes(const ses_solver* h, cudaStream_t s) {
 template <typename T>
 ses_status interior_unit(const ses_solver* h, bool mask, cudaStream_t s) {
     XProg p;
+    if (h->long1d) {  // [* conj W, inv y, V (M), fwd y, * W] [fwd x, K/N, inv x]
+        p.d_mid = DG_FULL;
+        p.m_mid = mask;
+        SES_TRY(pass_tw<T>(h, h->psi, h->psi, SM_TW_MID, p, s));
+        return pass_long_x<T>(h, s);
+    }
     if (h->last_axis == 0) {  // 1D: [V M, fwd, K/N, inv]
         p.mode = XM_1D;
         p.d_load = DG_FULL;
@@ -565,6 +605,24 @@ ses_status ensure_body(ses_solver* h, bool mask) {
 template <typename T>
 ses_status enqueue_steps(ses_solver* h, int S, bool mask) {
     cudaStream_t s = h->stream;
+    if (h->long1d) {
+        // [Vh, fwd y, * W] [x: fwd, K/N, inv] {[* conj W, inv y, V (M), fwd y, * W] [x]} ... [* conj W, inv y, Vh (M)]
+        XProg first;
+        first.d_load = DG_HALF;
+        SES_TRY(pass_tw<T>(h, h->psi, h->psi, SM_TW_START, first, s));
+        SES_TRY(pass_long_x<T>(h, s));
+        int interior = S - 1;
+        if (interior >= kBodyUnroll) SES_TRY(ensure_body<T>(h, mask));
+        while (interior >= kBodyUnroll) {
+            SES_CU(cudaGraphLaunch(h->body[mask ? 1 : 0], s));
+            interior -= kBodyUnroll;
+        }
+        for (; interior > 0; --interior) SES_TRY(interior_unit<T>(h, mask, s));
+        XProg last;
+        last.d_store = DG_HALF;
+        last.m_store = mask;
+        return pass_tw<T>(h, h->psi, h->psi, SM_TW_END, last, s);
+    }
     if (h->last_axis == 0) {
         // 1D batch: [Vh] U [V M] U ... U [Vh M], each step one fused x pass
         XProg first;
@@ -634,16 +692,16 @@ ses_status enqueue_observe(ses_solver* h, double xlo, double xhi) {
     cudaStream_t s = h->stream;
     ObsArgs o{};
     o.N = h->N;
-    o.nx = h->n[0];
-    o.ny = h->n[1];
-    o.fnx = make_fastdiv((uint32_t)h->n[0]);
-    o.fny = make_fastdiv((uint32_t)h->n[1]);
+    o.nx = phys_n(h, 0);
+    o.ny = phys_n(h, 1);
+    o.fnx = make_fastdiv((uint32_t)o.nx);
+    o.fny = make_fastdiv((uint32_t)o.ny);
     o.x0 = h->box[0];
-    o.hx = (h->box[1] - h->box[0]) / h->n[0];
+    o.hx = (h->box[1] - h->box[0]) / phys_n(h, 0);
     o.y0 = h->box[2];
-    o.hy = (h->box[3] - h->box[2]) / h->n[1];
+    o.hy = (h->box[3] - h->box[2]) / phys_n(h, 1);
     o.z0 = h->box[4];
-    o.hz = (h->box[5] - h->box[4]) / h->n[2];
+    o.hz = (h->box[5] - h->box[4]) / phys_n(h, 2);
     o.xlo = xlo;
     o.xhi = xhi;
     obs_real_kernel<T><<<kObsBlocks, 256, 0, s>>>(reinterpret_cast<const cx<T>*>(h->psi), h->V, o,
@@ -652,7 +710,14 @@ ses_status enqueue_observe(ses_solver* h, double xlo, double xhi) {
     SES_CU(cudaGetLastError());
     // k-space: phi = FFT(psi) into the scratch field, reduced in the last pass
     unsigned rows = 0;
-    if (h->last_axis == 0) {
+    if (h->long1d) {  // k-space copy: [fwd y, * W] into scratch, then [fwd x] reduced
+        XProg none;
+        SES_TRY(pass_tw<T>(h, h->psi, h->scratch, SM_TW_START, none, s));
+        XProg p;
+        p.mode = XM_REDUCE;
+        SES_TRY(pass_x<T>(h, h->scratch, h->scratch, p, s));
+        rows = h->pp[0].cgrid;
+    } else if (h->last_axis == 0) {
         XProg p;
         p.mode = XM_REDUCE;
         SES_TRY(pass_x<T>(h, h->psi, h->scratch, p, s));
@@ -902,6 +967,7 @@ ses_status autotune_impl(ses_solver* h, int flags) {
 template <typename T>
 std::string plan_info_t(const ses_solver* h) {
     std::ostringstream o;
+    if (h->long1d) o << "line of " << h->N << " as " << h->n[0] << " x " << h->n[1] << " (four-step): ";
     const char* names[3] = {"x", "y", "z"};
     for (int a = 0; a < 3; ++a) {
         o << names[a] << ":" << h->n[a];
@@ -1103,6 +1169,29 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
     }
     init_kernel_attrs();
 
+    // A 1D line longer than one CTA's transform (N > 4096) runs as N1 x N2 with
+    // compiled plans for both factors, N1 >= N2 as balanced as possible.
+    int long_n1 = 0, long_n2 = 0;
+    if (ax[1].n == 1 && ax[2].n == 1 && ax[0].n > 4096) {
+        const std::vector<int> lens = {16, 32, 48, 64, 96, 128, 160, 256, 512, 1024};
+        for (int n1 : lens) {
+            if (ax[0].n % n1) continue;
+            const int n2 = ax[0].n / n1;
+            if (n2 > n1) continue;
+            const bool ok = prec == SES_C128 ? (find_plan<double>(n1) && find_plan<double>(n2))
+                                             : (find_plan<float>(n1) && find_plan<float>(n2));
+            if (ok) {
+                long_n1 = n1;
+                long_n2 = n2;
+                break;
+            }
+        }
+        if (!long_n1)
+            return fail(SES_EINVAL, "1D line of " + std::to_string(ax[0].n) +
+                                        " points: lines above 4096 need N = N1 x N2 with both factors in "
+                                        "{16,32,48,64,96,128,160,256,512,1024}");
+    }
+
     ses_solver* h = new ses_solver();
     h->prec = prec;
     h->esize = prec == SES_C128 ? 16 : 8;
@@ -1114,6 +1203,11 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
         h->n[a] = ax[a].n;
         h->box[2 * a] = ax[a].xmin;
         h->box[2 * a + 1] = ax[a].xmax;
+    }
+    if (long_n1) {
+        h->long1d = true;
+        h->n[0] = long_n1;
+        h->n[1] = long_n2;
     }
     cudaGetDevice(&h->dev);
     h->last_axis = h->n[2] > 1 ? 2 : (h->n[1] > 1 ? 1 : 0);
@@ -1153,20 +1247,37 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
         return bail(fail(SES_ENOMEM, "pinned host allocation failed"));
     }
     for (int a = 0; a < 3; ++a) {
-        const int n = h->n[a];
-        if ((st = dalloc(h, &h->tw[a], (size_t)n * h->esize)) != SES_OK) return bail(st);
+        // wavenumber / kinetic tables follow the physical axis (a long line's x
+        // tables cover the whole line); FFT twiddles follow the layout axis
+        const int n = std::max(h->n[a], phys_n(h, a));
+        const int nl = h->n[a];
+        if ((st = dalloc(h, &h->tw[a], (size_t)nl * h->esize)) != SES_OK) return bail(st);
         if ((st = dalloc(h, (void**)&h->kv[a], (size_t)n * sizeof(double))) != SES_OK) return bail(st);
         if ((st = dalloc(h, (void**)&h->kd[a], (size_t)n * sizeof(cx<double>))) != SES_OK) return bail(st);
         const unsigned gb = (unsigned)((n + 255) / 256);
         if (prec == SES_C128)
-            build_twiddles<double><<<gb, 256, 0, h->stream>>>(n, reinterpret_cast<cx<double>*>(h->tw[a]));
+            build_twiddles<double><<<gb, 256, 0, h->stream>>>(nl, reinterpret_cast<cx<double>*>(h->tw[a]));
         else
-            build_twiddles<float><<<gb, 256, 0, h->stream>>>(n, reinterpret_cast<cx<float>*>(h->tw[a]));
+            build_twiddles<float><<<gb, 256, 0, h->stream>>>(nl, reinterpret_cast<cx<float>*>(h->tw[a]));
         build_axis_tables<<<gb, 256, 0, h->stream>>>(h->box[2 * a], h->box[2 * a + 1], n,
                                                      with_tables ? dt : 0.0,
                                                      with_tables ? mass : 1.0, h->kv[a], h->kd[a]);
         if ((st = dalloc(h, (void**)&h->kdf[a], (size_t)n * sizeof(cx<float>))) != SES_OK) return bail(st);
         convert_kernel<double, float><<<gb, 256, 0, h->stream>>>(h->kd[a], h->kdf[a], n);
+    }
+    if (h->long1d) {
+        if ((st = dalloc(h, &h->kfull, N * h->esize)) != SES_OK) return bail(st);
+        if ((st = dalloc(h, &h->tw4, N * h->esize)) != SES_OK) return bail(st);
+        if (prec == SES_C64 && (st = dalloc(h, &h->tw4l, N * h->esize)) != SES_OK) return bail(st);
+        const unsigned gb = (unsigned)std::min<long long>((N + 255) / 256, 148 * 16);
+        const double dtk = with_tables ? dt : 0.0, mk_ = with_tables ? mass : 1.0;
+        if (prec == SES_C128)
+            build_long_tables<double><<<gb, 256, 0, h->stream>>>(h->kv[0], h->n[0], h->n[1], dtk, mk_,
+                                                                 (cx<double>*)h->kfull, (cx<double>*)h->tw4, nullptr);
+        else
+            build_long_tables<float><<<gb, 256, 0, h->stream>>>(h->kv[0], h->n[0], h->n[1], dtk, mk_,
+                                                                (cx<float>*)h->kfull, (cx<float>*)h->tw4,
+                                                                (cx<float>*)h->tw4l);
     }
     if (cudaGetLastError() != cudaSuccess) return bail(fail(SES_EDEVICE, "axis table build failed"));
     if ((st = upload_stage_twiddles(h)) != SES_OK) return bail(st);
@@ -1207,8 +1318,8 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
 void finish_observe(const ses_solver* h, ses_observables* out) {
     const double* r = h->hsums;
     const double* k = h->hsums + kRedR;
-    const double dv = ((h->box[1] - h->box[0]) / h->n[0]) * ((h->box[3] - h->box[2]) / h->n[1]) *
-                      ((h->box[5] - h->box[4]) / h->n[2]);
+    const double dv = ((h->box[1] - h->box[0]) / phys_n(h, 0)) * ((h->box[3] - h->box[2]) / phys_n(h, 1)) *
+                      ((h->box[5] - h->box[4]) / phys_n(h, 2));
     auto ratio = [](double num, double den) { return den > 0.0 ? num / den : 0.0; };
     out->norm = r[0] * dv;
     out->energy_v = ratio(r[1], r[0]);
@@ -1341,6 +1452,7 @@ ses_status batch_wait(ses_batch_s* b, int timeout_ms) {
 template <typename T>
 bool class_has_batch_kernels(const BatchClass& c) {
     const ses_solver* h = c.mem[0];
+    if (h->long1d) return false;  // long lines step member by member
     for (int a = 0; a < 3; ++a) {
         if (h->n[a] < 2 && a > 0) continue;
         if (h->n[a] < 2) return false;  // a 1-point x axis has no compiled plan
@@ -1793,6 +1905,11 @@ ses_status ses_gpu_set_absorber_separable(ses_handle h, const double* mx, const 
     SES_TRY(check_handle(h));
     const double* m[3] = {mx, my, mz};
     if (!mx || !my || !mz) return fail(SES_EINVAL, "null mask profile");
+    if (h->long1d) {  // stored in full: the layout axes are not the line's axis
+        std::vector<double> full((size_t)h->N);
+        for (long long i = 0; i < h->N; ++i) full[(size_t)i] = (mx[i] * my[0]) * mz[0];
+        return ses_gpu_set_absorber(h, full.data());
+    }
     SES_TRY(wait_bounded(h, 0));
     drop_graphs(h);
     if (h->maskfull) {
@@ -1821,11 +1938,12 @@ ses_status ses_gpu_set_absorber(ses_handle h, const double* mask) {
     // Detect an exact per-axis product mask[i,j,k] == (mx[i]*my[j])*mz[k]:
     // profiles read off the axis lines through the cell of largest mask value.
     const int nx = h->n[0], ny = h->n[1], nz = h->n[2];
+    const bool try_separable = !h->long1d;
     long long best = 0;
     for (long long f = 1; f < h->N; ++f)
         if (mask[f] > mask[best]) best = f;
     const int bi = (int)(best % nx), bj = (int)((best / nx) % ny), bk = (int)(best / ((long long)nx * ny));
-    bool separable = mask[best] == 1.0;
+    bool separable = try_separable && mask[best] == 1.0;
     std::vector<double> mx(nx), my(ny), mz(nz);
     if (separable) {
         for (int i = 0; i < nx; ++i) mx[i] = mask[i + (long long)nx * (bj + (long long)ny * bk)];
@@ -1865,6 +1983,9 @@ ses_status ses_gpu_step(ses_handle h, int nsteps, int absorb) {
 ses_status ses_gpu_fft3(ses_handle h, int direction) {
     SES_TRY(check_handle(h));
     if (direction != 0 && direction != 1) return fail(SES_EINVAL, "direction must be 0 or 1");
+    if (h->long1d)
+        return fail(SES_EINVAL, "lines above 4096 points are transformed only inside the step (four-step "
+                                "layout); no natural-order FFT of them");
     return h->prec == SES_C128 ? enqueue_fft3<double>(h, h->psi, direction)
                                : enqueue_fft3<float>(h, h->psi, direction);
 }
@@ -1882,7 +2003,7 @@ ses_status ses_gpu_tables(ses_handle h, double* half_v, double* kin) {
         return st;
     }
     const unsigned gb = (unsigned)std::min<long long>((h->N + 255) / 256, 148 * 32);
-    build_full_tables<<<gb, 256, 0, h->stream>>>(h->V, h->kv[0], h->kv[1], h->kv[2], h->n[0], h->n[1],
+    build_full_tables<<<gb, 256, 0, h->stream>>>(h->V, h->kv[0], h->kv[1], h->kv[2], phys_n(h, 0), phys_n(h, 1),
                                                  h->N, h->dt, h->mass, (cx<double>*)dh, (cx<double>*)dk);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && dh) e = cudaMemcpyAsync(half_v, dh, bytes, cudaMemcpyDeviceToHost, h->stream);
@@ -1985,6 +2106,7 @@ ses_status ses_gpu_profile_step(ses_handle h, int nsteps, int absorb, double* pa
     if (!pass_ms) return fail(SES_EINVAL, "null output");
     if (!h->with_tables) return fail(SES_EINVAL, "handle has no phase tables");
     if (nsteps < 1) return fail(SES_EINVAL, "nsteps must be >= 1");
+    if (h->long1d) return fail(SES_EINVAL, "per-pass profile is not available for long 1D lines");
     for (int k = 0; k < 8; ++k) pass_ms[k] = 0.0;
     const bool mask = absorb != 0 && h->has_mask;
     return h->prec == SES_C128 ? profile_batch<double>(h, nsteps, mask, pass_ms)
@@ -1994,6 +2116,7 @@ ses_status ses_gpu_profile_step(ses_handle h, int nsteps, int absorb, double* pa
 ses_status ses_gpu_autotune(ses_handle h, int flags) {
     SES_TRY(check_handle(h));
     SES_TRY(wait_bounded(h, 0));
+    if (h->long1d) return SES_OK;  // long lines run the register-path kernels only
     return h->prec == SES_C128 ? autotune_impl<double>(h, flags) : autotune_impl<float>(h, flags);
 }
 

@@ -39,6 +39,11 @@ struct Tables {
     const cx<float>* kdf[3];
     double inv_mass;
     double kscale;             // 1/N, folded into the kinetic multiply
+    // long 1D line (four-step layout N1 x N2); null / 0 otherwise
+    const void* kfull;         // kinetic delta per stored k-space element (cx<T>)
+    const void* tw4;           // W_N^{n1 k2} per element (cx<T>; complex64: FP32-rounded)
+    const void* tw4l;          // complex64: FP32 remainder of tw4
+    int long_n2;               // N2: stored element (k1, k2) is frequency k2 + N2 k1
 };
 
 // complex64 phase multiplies in FP32 on the delta form: psi + psi*d, d = factor - 1.
@@ -74,14 +79,11 @@ struct PassArgs {
     double* partials;
 };
 
-// Absorber value at flat index f, coordinates (i, j, k): m = mx[i] * (my[j] * mz[k])
-// (complex64 path: FP32 product of mx[i] and the FP32-rounded line factor).
+// Absorber value at flat index f, coordinates (i, j, k): m = mx[i] * (my[j] * mz[k]), in FP64.
 template <typename T>
 __device__ __forceinline__ double maskval(const Tables& tb, long long f, int i, int j, int k) {
     if (tb.maskfull) return tb.maskfull[f];
-    const double lyz = tb.mask1[1][j] * tb.mask1[2][k];
-    if constexpr (sizeof(T) == 4) return (double)(tb.mask1f[0][i] * (float)lyz);
-    else return tb.mask1[0][i] * lyz;
+    return tb.mask1[0][i] * (tb.mask1[1][j] * tb.mask1[2][k]);
 }
 
 template <typename T>
@@ -108,9 +110,9 @@ __device__ __forceinline__ cx<T> apply_diag_tv(cx<T> v, int kind, cx<T> tab, int
     if constexpr (sizeof(T) == 4) {
         cx<float> p = v;
         if (kind != DG_NONE) p = add_mul(p, tab);
-        if (use_mask) {
-            const float mf = (float)m;
-            p = mk<float>(p.x * mf, p.y * mf);
+        if (use_mask) {  // p - p (1 - m): the FP32 rounding falls on the small 1 - m, not on m
+            const float md = (float)(1.0 - m);
+            p = mk<float>(fmaf(-p.x, md, p.x), fmaf(-p.y, md, p.y));
         }
         if (kind == DG_FULL) p = add_mul(p, tab);
         return p;
@@ -128,15 +130,14 @@ __device__ __forceinline__ double mask_at(const Tables& tb, long long f, int i, 
 }
 
 // psi_k * K / N then conj (inverse FFT start); complex64: FP32 on the delta form.
-__device__ __forceinline__ cx<float> kinetic_conj_f(cx<float> v, cx<float> d, float kscale) {
-    const cx<float> p = add_mul(v, d);
-    return mk<float>(p.x * kscale, -p.y * kscale);
+__device__ __forceinline__ cx<float> kinetic_conj_f(cx<float> v, cx<float> d, double kscale) {
+    return cconj(scale_d(add_mul(v, d), kscale));
 }
 
 template <typename T>
 __device__ __forceinline__ cx<T> kinetic_apply(cx<T> v, cx<double> dother, const cx<double>* kda64,
                                                const cx<float>* kda32, int pos, double kscale) {
-    if constexpr (sizeof(T) == 4) return kinetic_conj_f(v, dmul1f(narrow<float>(dother), kda32[pos]), (float)kscale);
+    if constexpr (sizeof(T) == 4) return kinetic_conj_f(v, dmul1f(narrow<float>(dother), kda32[pos]), kscale);
     else return kinetic_conj(v, dmul1(dother, kda64[pos]), kscale);
 }
 
@@ -147,6 +148,15 @@ __device__ __forceinline__ cx<T> kinetic_conj(cx<T> v, cx<double> d, double ksca
     cx<double> p = widen(v);
     p = p + p * d;
     return narrow<T>(mk<double>(p.x * kscale, -p.y * kscale));
+}
+
+// Kinetic multiply from a per-element delta table (long 1D lines).
+template <typename T>
+__device__ __forceinline__ cx<T> kinetic_full(cx<T> v, const void* kfull, long long idx, double kscale) {
+    if constexpr (sizeof(T) == 4)
+        return kinetic_conj_f(v, reinterpret_cast<const cx<float>*>(kfull)[idx], kscale);
+    else
+        return kinetic_conj(v, reinterpret_cast<const cx<double>*>(kfull)[idx], kscale);
 }
 
 // Kinetic multiply of element `pos` of an axis whose other two axes give the
@@ -206,7 +216,21 @@ enum XMode : int {
     XM_1D = 5,      // V/2 or V (* M), fwd x, K/N, inv x, [V/2 (* M)]   (x only axis)
     XM_REDUCE = 6   // fwd x, k-space sums                     (1D energy)
 };
-enum SModeK : int { SM_FWD = 0, SM_INV = 1, SM_FUSED = 2, SM_REDUCE = 3 };
+// Strided programs.  SM_TW_* are the strided halves of a long 1D line run as a
+// four-step transform (line of N = N1 N2 points stored as N1 x N2, x fastest):
+// the y pass is the length-N2 transform with the twiddles W_N^{n1 k2} on its
+// k-space side, the x pass (XM_1D) the length-N1 transform with the kinetic
+// phase of frequency k2 + N2 k1 between forward and inverse.
+enum SModeK : int {
+    SM_FWD = 0,       // fwd y/z
+    SM_INV = 1,       // inv y/z, scaled
+    SM_FUSED = 2,     // fwd, K/N, inv                 (last axis)
+    SM_REDUCE = 3,    // fwd, k-space sums
+    SM_TW_START = 4,  // [V/2 (* M)], fwd y, * W        (long line: batch start, or k-space copy)
+    SM_TW_MID = 5,    // * conj W, inv y, V (* M), fwd y, * W   (between steps)
+    SM_TW_END = 6     // * conj W, inv y, V/2 (* M)     (batch end)
+};
+constexpr int kSModes = 7;
 
 // ---------------------------------------------------------------------------
 // Contiguous-axis (x) pass.  Tile = L consecutive x-lines, loaded and stored
@@ -249,10 +273,9 @@ __global__ void __launch_bounds__(512, 1) xpass_kernel(const PassArgs<T> a) {
     auto sts = [&](int l, int e, cx<T> v) { sm[l * g.ls + e] = v; };
 
     if constexpr (MODE == XM_INV || MODE == XM_MID || MODE == XM_END) {
-        const T s = (T)a.out_scale;
         auto ldc = [&](int l, int e) -> cx<T> { return cconj(sm[l * g.ls + e]); };
         auto stc = [&](int l, int e, cx<T> v) {
-            sm[l * g.ls + e] = MODE == XM_INV ? scale(cconj(v), s) : cconj(v);
+            sm[l * g.ls + e] = MODE == XM_INV ? scale_d(cconj(v), a.out_scale) : cconj(v);
         };
         fft_tile<T, kEPTDev, false, false>(g, sm, a.tw, ldc, stc);
     }
@@ -392,9 +415,8 @@ __global__ void __launch_bounds__(512, 1) spass_kernel(const PassArgs<T> a) {
     if constexpr (MODE == SM_FWD) {
         fft_tile<T, kEPTDev, true, true>(g, sm, a.tw, ldg, stg);
     } else if constexpr (MODE == SM_INV) {
-        const T s = (T)a.out_scale;
         auto ldc = [&](int l, int e) -> cx<T> { return cconj(ldg(l, e)); };
-        auto stc = [&](int l, int e, cx<T> v) { stg(l, e, scale(cconj(v), s)); };
+        auto stc = [&](int l, int e, cx<T> v) { stg(l, e, scale_d(cconj(v), a.out_scale)); };
         fft_tile<T, kEPTDev, true, true>(g, sm, a.tw, ldc, stc);
     } else if constexpr (MODE == SM_FUSED) {
         auto stk = [&](int l, int e, cx<T> v) {

@@ -28,6 +28,12 @@ __device__ __forceinline__ cx<T> twmul(cx<T> v, const cx<T>* __restrict__ hi,
     }
 }
 
+// Four-step twiddle W_N^{n1 k2} of element f (long 1D lines).
+template <typename T>
+__device__ __forceinline__ cx<T> tw4_mul(cx<T> v, const Tables& tb, long long f) {
+    return twmul(v, reinterpret_cast<const cx<T>*>(tb.tw4), reinterpret_cast<const cx<T>*>(tb.tw4l), (int)f);
+}
+
 // Offset of stage p's table: tables are R_p x Ns_p entries, w^{r k N/(Ns R)} at [r*Ns + k].
 template <int R0, int R1, int R2>
 struct StageOff {
@@ -197,7 +203,9 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
 #pragma unroll
                 for (int r = 0; r < RL; ++r) {
                     const int pos = q + TL * b + r * (N / RL);
-                    const double k3[3] = {a.tb.kv[0][pos], a.tb.kv[1][jy], a.tb.kv[2][kz]};
+                    const int n2 = a.tb.long_n2;  // long line: element (pos, jy) is frequency jy + N2 pos
+                    const double k3[3] = {n2 ? a.tb.kv[0][jy + n2 * pos] : a.tb.kv[0][pos],
+                                          n2 ? 0.0 : a.tb.kv[1][jy], n2 ? 0.0 : a.tb.kv[2][kz]};
                     const cx<double> p = widen(v[b * RL + r]);
                     acc_k(acc, p.x * p.x + p.y * p.y, k3, a.tb.inv_mass);
                 }
@@ -206,7 +214,6 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
         return;
     }
     if constexpr (MODE == XM_FWD || MODE == XM_START || MODE == XM_INV || MODE == XM_END) {
-        const T sc = (T)a.out_scale;
         if (valid) {
 #pragma unroll
             for (int b = 0; b < E / RL; ++b)
@@ -214,7 +221,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
                 for (int r = 0; r < RL; ++r) {
                     const int pos = q + TL * b + r * (N / RL);
                     cx<T> e = v[b * RL + r];
-                    if constexpr (MODE == XM_INV) e = scale(cconj(e), sc);
+                    if constexpr (MODE == XM_INV) e = scale_d(cconj(e), a.out_scale);
                     if constexpr (MODE == XM_END) {
                         e = cconj(e);
                         if (a.d_store != DG_NONE || a.m_store)
@@ -238,6 +245,8 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
                     e = cconj(e);
                     if (a.d_mid != DG_NONE || a.m_mid)
                         e = apply_diag(e, a.d_mid, a.m_mid, mc * N + pos, pos, jy, kz, a.tb);
+                } else if (a.tb.kfull) {  // long line: kinetic of frequency k2 + N2 k1
+                    e = kinetic_full<T>(e, a.tb.kfull, mc * N + pos, a.tb.kscale);
                 } else {
                     e = kinetic_apply(e, dyz, a.tb.kd[0], a.tb.kdf[0], pos, a.tb.kscale);
                 }
@@ -278,7 +287,11 @@ template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, cla
 __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* tile) {
     constexpr int TL = N / E;
     using S = PlanShape<R0, R1, R2>;
-    constexpr int RL = S::last;
+    // SM_TW_START runs its FFT in the reversed radix order (the order of the
+    // second FFT of SM_TW_MID), like the contiguous batch-start pass.
+    constexpr bool kRev = MODE == SM_TW_START;
+    constexpr int RF = kRev ? S::last : R0;
+    constexpr int RL = kRev ? R0 : S::last;
     const int l = threadIdx.x % L, q = threadIdx.x / L;
     const long long s = blk * L + l;
     const bool valid = s < a.nlines;
@@ -287,20 +300,6 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
     const long long u = sc_ - w * a.nu;
     const long long base = u + w * a.sw;
     const long long se = a.se;
-    XchCta<T, L> x{tile, l};
-    cx<T> v[E];
-    constexpr bool kConjIn = MODE == SM_INV;
-#pragma unroll
-    for (int b = 0; b < E / R0; ++b)
-#pragma unroll
-        for (int r = 0; r < R0; ++r) {
-            const int pos = q + TL * b + r * (N / R0);
-            const cx<T> e = valid ? a.src[base + pos * se] : czero<T>();
-            v[b * R0 + r] = kConjIn ? cconj(e) : e;
-        }
-
-    rfft_plan<T, N, E, R0, R1, R2, false>(v, q, a.stw, a.stwl, x);
-
     const bool ypass = a.axis == 1;
     int c1, c2;  // the line's other two coordinates: y-pass (x, z), z-pass (x, y)
     if (ypass) {
@@ -309,6 +308,71 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
     } else {
         c2 = (int)fdiv((uint32_t)u, a.fnx);
         c1 = (int)(u - (long long)c2 * a.nx);
+    }
+    // potential / mask at element pos of this line (coordinates i, j, k)
+    auto diag = [&](cx<T> e, int kind, int msk, int pos) {
+        const long long f = base + pos * se;
+        return ypass ? apply_diag(e, kind, msk, f, c1, pos, c2, a.tb) : apply_diag(e, kind, msk, f, c1, c2, pos, a.tb);
+    };
+    XchCta<T, L> x{tile, l};
+    cx<T> v[E];
+#pragma unroll
+    for (int b = 0; b < E / RF; ++b)
+#pragma unroll
+        for (int r = 0; r < RF; ++r) {
+            const int pos = q + TL * b + r * (N / RF);
+            cx<T> e = valid ? a.src[base + pos * se] : czero<T>();
+            if constexpr (MODE == SM_INV) e = cconj(e);
+            if constexpr (MODE == SM_TW_START) {
+                if (a.d_load != DG_NONE || a.m_load) e = diag(e, a.d_load, a.m_load, pos);
+            }
+            if constexpr (MODE == SM_TW_MID || MODE == SM_TW_END)  // conj(e * conj W) = conj(e) * W
+                e = tw4_mul<T>(cconj(e), a.tb, base + pos * se);
+            v[b * RF + r] = e;
+        }
+
+    rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, a.stw, a.stwl, x);
+
+    if constexpr (MODE == SM_TW_START || MODE == SM_TW_END) {
+        if (valid) {
+#pragma unroll
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const int pos = q + TL * b + r * (N / RL);
+                    cx<T> e = v[b * RL + r];
+                    if constexpr (MODE == SM_TW_START) {
+                        e = tw4_mul<T>(e, a.tb, base + pos * se);
+                    } else {
+                        e = cconj(e);
+                        if (a.d_store != DG_NONE || a.m_store) e = diag(e, a.d_store, a.m_store, pos);
+                    }
+                    a.dst[base + pos * se] = e;
+                }
+        }
+        return;
+    }
+    if constexpr (MODE == SM_TW_MID) {
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int pos = q + TL * b + r * (N / RL);
+                cx<T> e = cconj(v[b * RL + r]);
+                if (a.d_mid != DG_NONE || a.m_mid) e = diag(e, a.d_mid, a.m_mid, pos);
+                v[b * RL + r] = e;
+            }
+        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+        if (valid) {
+#pragma unroll
+            for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+                for (int r = 0; r < R0; ++r) {
+                    const int pos = q + TL * b + r * (N / R0);
+                    a.dst[base + pos * se] = tw4_mul<T>(v[b * R0 + r], a.tb, base + pos * se);
+                }
+        }
+        return;
     }
 
     if constexpr (MODE == SM_REDUCE) {
@@ -331,7 +395,6 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
         return;
     }
     if constexpr (MODE == SM_FWD || MODE == SM_INV) {
-        const T scl = (T)a.out_scale;
         if (valid) {
 #pragma unroll
             for (int b = 0; b < E / RL; ++b)
@@ -339,7 +402,7 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
                 for (int r = 0; r < RL; ++r) {
                     const int pos = q + TL * b + r * (N / RL);
                     cx<T> e = v[b * RL + r];
-                    if constexpr (MODE == SM_INV) e = scale(cconj(e), scl);
+                    if constexpr (MODE == SM_INV) e = scale_d(cconj(e), a.out_scale);
                     a.dst[base + pos * se] = e;
                 }
         }

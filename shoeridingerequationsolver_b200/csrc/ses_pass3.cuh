@@ -145,7 +145,6 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
             c1 = (int)(u - (long long)c2 * a.nx);
         }
         if constexpr (MODE == SM_FWD || MODE == SM_INV) {
-            const T scl = (T)a.out_scale;
             if (valid) {
 #pragma unroll
                 for (int b = 0; b < E / RL; ++b)
@@ -153,7 +152,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
                     for (int r = 0; r < RL; ++r) {
                         const int pos = q + TL * b + r * (N / RL);
                         cx<T> e = v[b * RL + r];
-                        if constexpr (MODE == SM_INV) e = scale(cconj(e), scl);
+                        if constexpr (MODE == SM_INV) e = scale_d(cconj(e), a.out_scale);
                         a.dst[base + pos * a.se] = e;
                     }
             }
@@ -272,11 +271,9 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
         // separable absorber: per-line factor my[j] * mz[k] (the mask is m = mx[i] * (my[j] * mz[k]))
         const bool sep = a.tb.maskfull == nullptr && a.tb.mask1[0] != nullptr;
         const double myz = sep ? a.tb.mask1[1][jy] * a.tb.mask1[2][kz] : 1.0;
-        const float myzf = (float)myz;
         auto mval = [&](int pos) -> double {  // == maskval<T>(a.tb, mc * N + pos, pos, jy, kz)
             if (!sep) return a.tb.maskfull ? a.tb.maskfull[mc * N + pos] : 1.0;
-            if constexpr (sizeof(T) == 4) return (double)(a.tb.mask1f[0][pos] * myzf);
-            else return a.tb.mask1[0][pos] * myz;
+            return a.tb.mask1[0][pos] * myz;
         };
         cx<T>* line = ptile + (size_t)lc * N;
         const cx<T>* tline = ttile + (size_t)lc * N;

@@ -19,7 +19,7 @@ struct PlanEntry {
     int ls = 0;             // lines per strided-pass CTA
     int xw = 4;             // warps per contiguous-pass CTA
     PassKernel<T> xk[7];    // by XMode
-    PassKernel<T> sk[4];    // by SModeK
+    PassKernel<T> sk[kSModes];  // by SModeK
     // pipelined variants; the solver picks one per axis (default 0, or autotuned)
     using XPipe = void (*)(const PassArgs<T>, const PipeArgs);
     using SPipe = void (*)(const PassArgs<T>, const CUtensorMap, const PipeArgs);
@@ -35,21 +35,21 @@ struct PlanEntry {
         int bbps[7] = {0, 0, 0, 0, 0, 0, 0};
     };
     struct SVar {
-        SPipe k[4] = {nullptr, nullptr, nullptr, nullptr};
-        SBPipe kb[4] = {nullptr, nullptr, nullptr, nullptr};
+        SPipe k[kSModes] = {};
+        SBPipe kb[kSModes] = {};
         int ls = 0, nbuf = 0;
         size_t smem = 0;
-        int bps[4] = {0, 0, 0, 0};
-        int bbps[4] = {0, 0, 0, 0};
+        int bps[kSModes] = {};
+        int bbps[kSModes] = {};
     };
     std::vector<XVar> xv;
     std::vector<SVar> sv;
     // batched kernels (many fields of this length per launch), by mode
     using XBatch = void (*)(const PassArgs<T>*, const BatchWork);
     XBatch xb[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    XBatch sb[4] = {nullptr, nullptr, nullptr, nullptr};
+    XBatch sb[kSModes] = {};
     int xb_bps[7] = {0, 0, 0, 0, 0, 0, 0};  // resident CTAs per SM
-    int sb_bps[4] = {0, 0, 0, 0};
+    int sb_bps[kSModes] = {};
 };
 
 template <typename K>
@@ -78,6 +78,9 @@ PlanEntry<T> make_plan_entry() {
     p.sk[SM_INV] = spass2_kernel<T, SM_INV, N, E, R0, R1, R2, LS>;
     p.sk[SM_FUSED] = spass2_kernel<T, SM_FUSED, N, E, R0, R1, R2, LS>;
     p.sk[SM_REDUCE] = spass2_kernel<T, SM_REDUCE, N, E, R0, R1, R2, LS>;
+    p.sk[SM_TW_START] = spass2_kernel<T, SM_TW_START, N, E, R0, R1, R2, LS>;
+    p.sk[SM_TW_MID] = spass2_kernel<T, SM_TW_MID, N, E, R0, R1, R2, LS>;
+    p.sk[SM_TW_END] = spass2_kernel<T, SM_TW_END, N, E, R0, R1, R2, LS>;
     const int smem = N * LS * (int)sizeof(cx<T>);
     for (auto k : p.sk) allow_smem(k, smem);
     p.xb[XM_START] = xbatch_kernel<T, XM_START, N, E, R0, R1, R2>;
@@ -91,7 +94,7 @@ PlanEntry<T> make_plan_entry() {
         if (p.xb[m])
             cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&p.xb_bps[m], p.xb[m], p.xw * 32, 0,
                                                                   cudaOccupancyDefault);
-    for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < kSModes; ++m)
         if (p.sb[m]) {
             allow_smem(p.sb[m], smem);
             cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&p.sb_bps[m], p.sb[m], LS * (N / E), smem,

@@ -217,3 +217,78 @@ def build_c4_instance(spec: dict) -> Workload:
     return Workload(f"c4_tunnel_{spec['n']}_{spec['index']}", g, barrier(g, spec["barrier"], -1.0, 1.0),
                     psi0, spec["dt"], spec["steps"], mask=mask_profiles(g, spec["mask_frac"]),
                     observe_every=100, x_range=(1.0, math.inf), meta=dict(spec))
+
+
+def config_c5_specs(count: int = 48, seed: int = SEED_BASE + 4) -> list[dict]:
+    """Serving stream: `count` requests, 40% 1D / 30% 2D / 30% 3D, steps log-uniform in
+    [100, 5000], dt U[0.002, 0.01], complex64, observables every 100 steps, cos^(1/8)
+    absorber on the outer 10% of each transformed axis.
+      1D: 65536 points on [-200, 200): Morse (depth U[0.5,10], alpha 0.5, x0 0), double well
+          (barrier U[0.5,10], a 3) or Poschl-Teller (depth U[0.5,10], a 1); packet sigma 1
+          at the well minimum, k0 = 0.5.
+      2D: 512^2 or 1024^2 on [-30, 30)^2: harmonic dot (omega U[0.2,1]) or stadium (R 13,
+          half-length 6.5, V = 50 outside); packet sigma 1.5 at the origin, k0 = (2, 0).
+      3D: n in {64, 128, 256}: harmonic (omega U[0.5,2], box [-10,10)) or regularized
+          Coulomb Z = 1 (box [-40,40)); packet sigma 1 at (1, 0, 0) (harmonic) or sigma 1.5
+          at (2, 0, 0) (Coulomb), at rest.
+    Drawn per request in this order: kind, variant, size, strength, steps, dt."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        u = float(rng.uniform())
+        kind = "1d" if u < 0.4 else ("2d" if u < 0.7 else "3d")
+        variant = int(rng.integers(0, 3 if kind == "1d" else 2))
+        size = int(rng.integers(0, 2 if kind == "2d" else 3))
+        strength = float(rng.uniform())
+        steps = int(round(math.exp(rng.uniform(math.log(100.0), math.log(5000.0)))))
+        dt = float(rng.uniform(0.002, 0.01))
+        if kind == "1d":
+            pot = ("morse", "double_well", "poschl_teller")[variant]
+            dims, val = (65536, 1, 1), 0.5 + 9.5 * strength
+        elif kind == "2d":
+            pot = ("harmonic", "stadium")[variant]
+            n = (512, 1024)[size]
+            dims, val = (n, n, 1), 0.2 + 0.8 * strength
+        else:
+            pot = ("harmonic", "coulomb")[variant]
+            n = (64, 128, 256)[size]
+            dims, val = (n, n, n), 0.5 + 1.5 * strength
+        out.append({"index": i, "kind": kind, "potential": pot, "dims": dims, "strength": val,
+                    "steps": steps, "dt": dt, "points": dims[0] * dims[1] * dims[2]})
+    return out
+
+
+def build_c5_request(spec: dict) -> dict:
+    """Keyword arguments of Server.submit for one serving request."""
+    from .core import line_grid
+    kind, pot, v = spec["kind"], spec["potential"], spec["strength"]
+    if kind == "1d":
+        g1 = Grid1D(-200.0, 200.0, spec["dims"][0])
+        if pot == "morse":
+            V, x0 = morse(g1, v, 0.5, 0.0), 0.0
+        elif pot == "double_well":
+            V, x0 = double_well(g1, v, 3.0), 3.0
+        else:
+            V, x0 = poschl_teller(g1, v, 1.0), 0.0
+        g = line_grid(g1)
+        psi = gaussian(g, (x0, 0.0, 0.0), (1.0, 1.0, 1.0), (0.5, 0.0, 0.0))
+    elif kind == "2d":
+        n = spec["dims"][0]
+        a = Grid1D(-30.0, 30.0, n)
+        g = Grid3D(a, a, Grid1D(0.0, 2.0, 1))
+        V = harmonic(g, v) if pot == "harmonic" else stadium(g, 6.5, 13.0, 50.0)
+        psi = gaussian(g, (0.0, 0.0, 0.0), (1.5, 1.5, 1.0), (2.0, 0.0, 0.0))
+    else:
+        n = spec["dims"][0]
+        if pot == "harmonic":
+            g = cube_grid(-10.0, 10.0, n)
+            V = harmonic(g, v)
+            psi = gaussian(g, (1.0, 0.0, 0.0), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0))
+        else:
+            g = cube_grid(-40.0, 40.0, n)
+            V = regularized_coulomb(g, 1.0)
+            psi = gaussian(g, (2.0, 0.0, 0.0), (1.5, 1.5, 1.5), (0.0, 0.0, 0.0))
+    mask = tuple(np.ones(1) if ax.n == 1 else mask_profile(ax, 0.1 * (ax.xmax - ax.xmin))
+                 for ax in (g.x, g.y, g.z))
+    return dict(grid=g, V=V, psi0=psi, dt=spec["dt"], nsteps=spec["steps"], observe_every=100, mask=mask,
+                precision="c64", x_range=(0.0, math.inf))

@@ -318,3 +318,24 @@ def test_serve_arguments_without_device():
         assert _abi.lib.ses_serve_close(s) == _abi.SES_OK
     else:
         assert st == _abi.SES_EDEVICE
+
+
+def test_four_step_layout_of_long_lines():
+    """Long 1D lines (ses_gpu.cu long1d, ses_pass2.cuh SM_TW_*): the stored
+    layout, twiddle index and frequency map of the four-step transform, modelled
+    with numpy on a 24 x 16 line and compared with the plain DFT."""
+    n1, n2 = 24, 16
+    N = n1 * n2
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    a = x.reshape(n2, n1)                               # a[n2, n1] = x[n1 + N1 n2]
+    y = np.fft.fft(a, axis=0)                           # y pass: length-N2 transforms -> [k2, n1]
+    f = np.arange(N).reshape(n2, n1)                    # flat index n1 + N1 k2 of each stored element
+    tw = np.exp(-2j * np.pi * (((f % n1) * (f // n1)) % N) / N)
+    z = np.fft.fft(y * tw, axis=1)                      # x pass: length-N1 transforms -> [k2, k1]
+    k1, k2 = f % n1, f // n1
+    X = np.fft.fft(x)
+    assert np.allclose(z, X[k2 + n2 * k1], atol=1e-9)   # stored (k1, k2) is frequency k2 + N2 k1
+    # inverse: conj trick with conj(W) before the y transforms, as the between-steps pass
+    back = np.conj(np.fft.fft(np.conj(np.conj(np.fft.fft(np.conj(z), axis=1)) / n1 * np.conj(tw)), axis=0)) / n2
+    assert np.allclose(back.reshape(-1), x, atol=1e-12)

@@ -85,7 +85,7 @@ def test_serve_alone_equals_mix_and_oracle(ses, oracle):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("dims", [(48, 48, 48), (64, 64, 64), (96, 96, 1), (256, 1, 1)])
+@pytest.mark.parametrize("dims", [(48, 48, 48), (64, 64, 64), (96, 96, 1), (256, 1, 1), (65536, 1, 1)])
 def test_step_calls_compose_exactly(ses, dims):
     """n steps in one call == the same n steps split over several calls (complex64)."""
     s = spec(ses, dims, 8.0, 30, nsteps=0, every=0)
