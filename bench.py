@@ -57,6 +57,7 @@ def parse_args(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=["c4", "c2", "c3", "c1"], default="c4")
     ap.add_argument("--instances", type=int, default=256, help="batched sweep size (c4)")
+    ap.add_argument("--sizes", default="", help="c4: keep only these grid sizes (comma list), for profiling")
     ap.add_argument("--n", type=int, default=0, help="grid size override for c1/c2/c3")
     ap.add_argument("--precision", choices=["c64", "c128"], default="c64")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -154,6 +155,14 @@ def full_mask(mask):
 # ---------------------------------------------------------------------------
 # C4: the batched sweep
 # ---------------------------------------------------------------------------
+def c4_specs(args):
+    from shoeridingerequationsolver_b200 import scenes
+    if not args.sizes:
+        return scenes.config_c4_specs(args.instances)
+    keep = {int(x) for x in args.sizes.split(",")}
+    return [s for s in scenes.config_c4_specs(256) if s["n"] in keep][:args.instances]
+
+
 def build_c4(ses, specs, prec="c64"):
     from shoeridingerequationsolver_b200 import scenes
     ops = []
@@ -456,7 +465,7 @@ def run_reference(args):
         return 0
     if args.config == "c4":
         from shoeridingerequationsolver_b200 import scenes
-        specs = scenes.config_c4_specs(args.instances)
+        specs = c4_specs(args)
         cb = cpu_baseline_c4(specs, budget_s=60.0)
         cfg = {"workload": f"c4_batched_tunnel_{args.instances}", "instances": args.instances,
                "sizes": sorted({s["n"] for s in specs}), "dt": 0.005, "precision": "c128 (FP64 CPU core)"}
@@ -547,7 +556,7 @@ def run_ours(args):
         return 0
 
     # ---- C4 batched sweep (headline) ----
-    specs = scenes.config_c4_specs(args.instances)
+    specs = c4_specs(args)
     npts = sum(sp["n"] ** 3 for sp in specs)
     t_build = time.perf_counter()
     ops = build_c4(ses, specs)
@@ -575,7 +584,8 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(W, 9),
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c64", "data": "synthetic",
-        "config": {"workload": f"c4_batched_tunnel_{args.instances}", "instances": args.instances,
+        "config": {"workload": f"c4_batched_tunnel_{len(specs)}" + (f"_sizes_{args.sizes}" if args.sizes else ""),
+                   "instances": len(specs),
                    "sizes": dict(sorted(Counter(sp["n"] for sp in specs).items())), "grid_points": npts,
                    "dt": 0.005, "precision": "complex64 fields, FP64-built tables, FP64 reductions",
                    "absorber": "cos^(1/8) on the outer 8%, after every step",
