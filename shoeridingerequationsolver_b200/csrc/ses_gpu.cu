@@ -1546,6 +1546,29 @@ ses_status class_maps(const BatchClass& c, int buf, CUtensorMap*& dmaps, size_t&
     return SES_OK;
 }
 
+// Members of a class share one copy of every table whose contents are equal,
+// so the batched passes keep one set in L1/L2 instead of one per instance:
+// the stage twiddles (same plan) always, and an axis's wavenumber / kinetic
+// tables when the axis extent, dt and mass are equal.
+template <typename T>
+void share_tables(const BatchClass& c, size_t i, PassArgs<T>& a) {
+    const ses_solver* h0 = c.mem[0];
+    const ses_solver* h = c.mem[i];
+    a.stw = reinterpret_cast<const cx<T>*>(h0->stw[a.axis]);
+    a.stwl = reinterpret_cast<const cx<T>*>(h0->stwl[a.axis]);
+    for (int ax = 0; ax < 3; ++ax)
+        for (size_t j = 0; j < i; ++j) {
+            const ses_solver* g = c.mem[j];
+            if (g->box[2 * ax + 1] - g->box[2 * ax] == h->box[2 * ax + 1] - h->box[2 * ax] && g->dt == h->dt &&
+                g->mass == h->mass) {
+                a.tb.kd[ax] = g->kd[ax];
+                a.tb.kdf[ax] = g->kdf[ax];
+                a.tb.kv[ax] = g->kv[ax];
+                break;
+            }
+        }
+}
+
 template <typename T>
 ses_status class_upload(const ses_batch_s* b, BatchClass& c) {
     const size_t nm = c.mem.size();
@@ -1579,6 +1602,7 @@ ses_status class_upload(const ses_batch_s* b, BatchClass& c) {
                 } else {
                     a = make_args<T>(h, 0, h->psi, h->psi);  // unused slot
                 }
+                share_tables(c, i, a);
             }
     class_select<T>(b, c);
     SES_TRY(class_maps(c, 0, c.dmaps, c.mcap));
@@ -1658,11 +1682,11 @@ ses_status class_launch(const ses_batch_s* b, const BatchClass& c, int prog, boo
     if (axis == 0) {
         const int bps = std::max(1, e->xb_bps[mode]);
         const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * bps));
-        e->xb[mode]<<<grid, pp.cblock, 0, s>>>(args, w);
+        e->xb[mode]<<<grid, pp.cblock, e->xbsm, s>>>(args, w);
     } else {
         const int bps = std::max(1, e->sb_bps[mode]);
         const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * bps));
-        e->sb[mode]<<<grid, pp.cblock, pp.csmem, s>>>(args, w);
+        e->sb[mode]<<<grid, pp.cblock, pp.csmem + e->twb, s>>>(args, w);
     }
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return fail(SES_EDEVICE, std::string("batched pass launch: ") + cudaGetErrorString(err));

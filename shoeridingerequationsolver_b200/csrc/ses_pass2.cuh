@@ -28,6 +28,16 @@ __device__ __forceinline__ cx<T> twmul(cx<T> v, const cx<T>* __restrict__ hi,
     }
 }
 
+// 16-byte asynchronous global -> shared copies (cp.async, L2 only), used to fetch
+// the potential-table rows of a tile while its first FFT runs.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // Four-step twiddle W_N^{n1 k2} of element f (long 1D lines).
 template <typename T>
 __device__ __forceinline__ cx<T> tw4_mul(cx<T> v, const Tables& tb, long long f) {
@@ -101,6 +111,27 @@ struct PlanShape {
     static constexpr int v1 = R2 > 1 ? R1 : (R1 > 1 ? R0 : 1);
     static constexpr int v2 = R2 > 1 ? R0 : 1;
     static constexpr int fwd_tables = R0 + (R1 > 1 ? R1 * R0 : 0) + (R2 > 1 ? R2 * R0 * R1 : 0);
+    static constexpr int rev_tables = v0 + (v1 > 1 ? v1 * v0 : 0) + (v2 > 1 ? v2 * v0 * v1 : 0);
+    static constexpr int tables = fwd_tables + rev_tables;
+};
+
+// Shared-memory copy of a plan's stage twiddles (forward then reversed tables;
+// complex64 also the lo parts) for persistent kernels: loaded once per CTA, so
+// the FFT stages read twiddles at shared-memory latency and the tables of
+// many instances do not compete for L1.
+template <typename T, int R0, int R1, int R2>
+struct TwStage {
+    static constexpr int count = PlanShape<R0, R1, R2>::tables;
+    static constexpr size_t bytes = (size_t)count * sizeof(cx<T>) * (sizeof(T) == 4 ? 2 : 1);
+    static __device__ __forceinline__ void load(cx<T>* dst, const cx<T>* hi, const cx<T>* lo) {
+        for (int i = threadIdx.x; i < count; i += blockDim.x) {
+            dst[i] = hi[i];
+            if constexpr (sizeof(T) == 4) dst[count + i] = lo[i];
+        }
+    }
+    static __device__ __forceinline__ const cx<T>* lo_of(const cx<T>* dst) {
+        return sizeof(T) == 4 ? dst + count : dst;
+    }
 };
 
 // FFT with the plan's own order (tables at 0) or reversed order (tables after).
@@ -151,8 +182,12 @@ struct XShape {
 // Body of the contiguous pass for CTA tile `blk` (NW * LPW lines); `a` is the
 // kernel parameter (single field) or an entry of a per-instance array in
 // global memory (batched passes).
+// vt (optional): shared memory for this CTA's potential-table rows (NW * LPW
+// lines of N entries); the between-steps and batch-end passes then fetch the
+// rows asynchronously at the start of the tile and read them after the first FFT.
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2, class A>
-__device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb) {
+__device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb, const cx<T>* twh,
+                                            const cx<T>* twl, cx<T>* vt = nullptr) {
     using XS = XShape<T, N, E>;
     constexpr int TL = XS::TL;
     constexpr int LPW = XS::LPW;
@@ -176,6 +211,33 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
     const cx<T>* src = a.src + mc * N;
     cx<T>* dst = a.dst + mc * N;
     cx<T> v[E];
+    constexpr bool kTabLate = MODE == XM_MID || MODE == XM_END;  // table used after the first FFT
+    cx<T>* vrow = vt ? vt + (size_t)(warp * LPW + lw) * N : nullptr;
+    if constexpr (kTabLate) {
+        const bool want = MODE == XM_MID ? a.d_mid != DG_NONE : a.d_store != DG_NONE;
+        if (vt && want) {  // this warp's rows, 16-byte chunks spread over the lanes
+            __syncwarp();  // the previous tile's reads of these rows are done
+            constexpr int CH = N * (int)sizeof(cx<T>) / 16;
+            const long long m0 = (blk * NW + warp) * LPW;
+            const cx<T>* tab = reinterpret_cast<const cx<T>*>(a.tb.vtab);
+            for (int c = lane; c < LPW * CH; c += 32) {
+                const int ln = c / CH, ch = c - ln * CH;
+                if (m0 + ln < a.nlines)
+                    cp_async16(reinterpret_cast<char*>(vt + (size_t)(warp * LPW + ln) * N) + 16 * ch,
+                               reinterpret_cast<const char*>(tab + (m0 + ln) * N) + 16 * ch);
+            }
+            cp_async_commit();
+        }
+    }
+    // potential / mask at element pos of this line; the table entry from vrow when prefetched
+    auto diag = [&](cx<T> e, int kind, int msk, int pos) {
+        const long long f = mc * N + pos;
+        if (vrow) {
+            const cx<T> tab = kind != DG_NONE ? vrow[pos] : e;
+            return apply_diag_tv(e, kind, tab, msk, msk ? maskval<T>(a.tb, f, pos, jy, kz) : 1.0);
+        }
+        return apply_diag(e, kind, msk, f, pos, jy, kz, a.tb);
+    };
 
     // load the first FFT's inputs (coalesced along the line)
     constexpr bool kConjIn = MODE == XM_INV || MODE == XM_MID || MODE == XM_END;
@@ -192,8 +254,14 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
             v[b * RF + r] = kConjIn ? cconj(e) : e;
         }
 
-    rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, a.stw, a.stwl, x);
+    rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, twh, twl, x);
     // v[b*RL + r] now at position q + TL b + r N/RL
+    if constexpr (kTabLate) {
+        if (vt) {
+            cp_async_wait_all();
+            __syncwarp();
+        }
+    }
 
     if constexpr (MODE == XM_REDUCE) {
         double acc[kRedK] = {0, 0, 0, 0, 0};
@@ -224,8 +292,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
                     if constexpr (MODE == XM_INV) e = scale_d(cconj(e), a.out_scale);
                     if constexpr (MODE == XM_END) {
                         e = cconj(e);
-                        if (a.d_store != DG_NONE || a.m_store)
-                            e = apply_diag(e, a.d_store, a.m_store, mc * N + pos, pos, jy, kz, a.tb);
+                        if (a.d_store != DG_NONE || a.m_store) e = diag(e, a.d_store, a.m_store, pos);
                     }
                     dst[pos] = e;
                 }
@@ -243,8 +310,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
                 cx<T> e = v[b * RL + r];
                 if constexpr (MODE == XM_MID) {
                     e = cconj(e);
-                    if (a.d_mid != DG_NONE || a.m_mid)
-                        e = apply_diag(e, a.d_mid, a.m_mid, mc * N + pos, pos, jy, kz, a.tb);
+                    if (a.d_mid != DG_NONE || a.m_mid) e = diag(e, a.d_mid, a.m_mid, pos);
                 } else if (a.tb.kfull) {  // long line: kinetic of frequency k2 + N2 k1
                     e = kinetic_full<T>(e, a.tb.kfull, mc * N + pos, a.tb.kscale);
                 } else {
@@ -252,7 +318,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
                 }
                 v[b * RL + r] = e;
             }
-        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
         // v[b*R0 + r] at position q + TL b + r N/R0
         if (valid) {
 #pragma unroll
@@ -276,7 +342,7 @@ template <typename T, int MODE, int N, int E, int R0, int R1, int R2>
 __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4) xpass2_kernel(const PassArgs<T> a) {
     using XS = XShape<T, N, E>;
     __shared__ cx<T> xb[XS::NW * XS::LPW * XS::PITCH];
-    xpass2_body<T, MODE, N, E, R0, R1, R2>(a, (long long)blockIdx.x, xb);
+    xpass2_body<T, MODE, N, E, R0, R1, R2>(a, (long long)blockIdx.x, xb, a.stw, a.stwl);
 }
 
 // ---------------------------------------------------------------------------
@@ -284,7 +350,8 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4) xpass2_kernel(con
 // line; thread (l = tid % L, q = tid / L).  Modes as in SModeK.
 // ---------------------------------------------------------------------------
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, class A>
-__device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* tile) {
+__device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* tile, const cx<T>* twh,
+                                            const cx<T>* twl) {
     constexpr int TL = N / E;
     using S = PlanShape<R0, R1, R2>;
     // SM_TW_START runs its FFT in the reversed radix order (the order of the
@@ -331,7 +398,7 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
             v[b * RF + r] = e;
         }
 
-    rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, a.stw, a.stwl, x);
+    rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, twh, twl, x);
 
     if constexpr (MODE == SM_TW_START || MODE == SM_TW_END) {
         if (valid) {
@@ -362,7 +429,7 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
                 if (a.d_mid != DG_NONE || a.m_mid) e = diag(e, a.d_mid, a.m_mid, pos);
                 v[b * RL + r] = e;
             }
-        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
         if (valid) {
 #pragma unroll
             for (int b = 0; b < E / R0; ++b)
@@ -419,7 +486,7 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
                 const int pos = q + TL * b + r * (N / RL);
                 v[b * RL + r] = kinetic_apply(v[b * RL + r], dother, kda, kdaf, pos, a.tb.kscale);
             }
-        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
         if (valid) {
 #pragma unroll
             for (int b = 0; b < E / R0; ++b)
@@ -435,7 +502,8 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L>
 __global__ void __launch_bounds__(L*(N / E), 1) spass2_kernel(const PassArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    spass2_body<T, MODE, N, E, R0, R1, R2, L>(a, (long long)blockIdx.x, reinterpret_cast<cx<T>*>(smraw));
+    spass2_body<T, MODE, N, E, R0, R1, R2, L>(a, (long long)blockIdx.x, reinterpret_cast<cx<T>*>(smraw), a.stw,
+                                              a.stwl);
 }
 
 // ---------------------------------------------------------------------------
@@ -454,21 +522,38 @@ template <typename T, int MODE, int N, int E, int R0, int R1, int R2>
 __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4)
     xbatch_kernel(const PassArgs<T>* __restrict__ args, const BatchWork w) {
     using XS = XShape<T, N, E>;
+    using TW = TwStage<T, R0, R1, R2>;
     __shared__ cx<T> xb[XS::NW * XS::LPW * XS::PITCH];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T>* tw = reinterpret_cast<cx<T>*>(smraw);
+    cx<T>* vt = reinterpret_cast<cx<T>*>(smraw + TW::bytes);  // XBatchSmem: rows of the potential table
+    if (blockIdx.x < w.total) TW::load(tw, args[0].stw, args[0].stwl);  // one plan per class
+    __syncthreads();
     for (uint32_t t = blockIdx.x; t < w.total; t += gridDim.x) {
         const uint32_t inst = fdiv(t, w.fbpi);
-        xpass2_body<T, MODE, N, E, R0, R1, R2>(args[inst], (long long)(t - inst * w.bpi), xb);
+        xpass2_body<T, MODE, N, E, R0, R1, R2>(args[inst], (long long)(t - inst * w.bpi), xb, tw, TW::lo_of(tw), vt);
     }
+}
+
+// Dynamic shared memory of xbatch_kernel: stage twiddles, then NW * LPW table rows.
+template <typename T, int N, int E, int R0, int R1, int R2>
+constexpr size_t xbatch_smem() {
+    return TwStage<T, R0, R1, R2>::bytes +
+           (size_t)XShape<T, N, E>::NW * XShape<T, N, E>::LPW * N * sizeof(cx<T>);
 }
 
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L>
 __global__ void __launch_bounds__(L*(N / E), 1)
     sbatch_kernel(const PassArgs<T>* __restrict__ args, const BatchWork w) {
+    using TW = TwStage<T, R0, R1, R2>;
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T>* tile = reinterpret_cast<cx<T>*>(smraw);
+    cx<T>* tw = tile + (size_t)N * L;
+    if (blockIdx.x < w.total) TW::load(tw, args[0].stw, args[0].stwl);
+    __syncthreads();
     for (uint32_t t = blockIdx.x; t < w.total; t += gridDim.x) {
         const uint32_t inst = fdiv(t, w.fbpi);
-        spass2_body<T, MODE, N, E, R0, R1, R2, L>(args[inst], (long long)(t - inst * w.bpi), tile);
+        spass2_body<T, MODE, N, E, R0, R1, R2, L>(args[inst], (long long)(t - inst * w.bpi), tile, tw, TW::lo_of(tw));
     }
 }
 

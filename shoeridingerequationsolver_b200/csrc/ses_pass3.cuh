@@ -21,6 +21,12 @@ struct PipeArgs {
     unsigned* err;      // device error word (bit 0: a bounded wait expired)
 };
 
+// Offset of the stage-twiddle copy: after the NBUF ring buffers and their
+// mbarriers, rounded up to 16 bytes.
+__host__ __device__ constexpr size_t pipe_tw_offset(size_t ring_bytes, int nbuf) {
+    return (ring_bytes + (size_t)nbuf * 8 + 15) / 16 * 16;
+}
+
 // XOR-swizzled position inside a dense line: bijective on [0, N) for N % 16 == 0,
 // spreads both exchange patterns of the compiled plans over the banks.
 __device__ __forceinline__ int swz(int pos) { return pos ^ ((pos >> 4) & 15); }
@@ -79,6 +85,9 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
     extern __shared__ __align__(1024) unsigned char smraw3[];
     cx<T>* tiles = reinterpret_cast<cx<T>*>(smraw3);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smraw3 + (size_t)NBUF * TILE_BYTES);
+    using TW = TwStage<T, R0, R1, R2>;
+    cx<T>* twh = reinterpret_cast<cx<T>*>(smraw3 + pipe_tw_offset((size_t)NBUF * TILE_BYTES, NBUF));
+    const cx<T>* twl = TW::lo_of(twh);
     const int l = threadIdx.x % L, q = threadIdx.x / L;
     const int nmine = blockIdx.x < (unsigned)pa.ntiles ? (pa.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
@@ -86,6 +95,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
         for (int b = 0; b < NBUF; ++b) mbar_init(smem_u32(&bars[b]), 1);
         fence_mbar_init();
     }
+    if (nmine > 0) TW::load(twh, f.args(blockIdx.x).stw, f.args(blockIdx.x).stwl);
     __syncthreads();
     auto issue = [&](int i) {  // thread 0: load this CTA's i-th tile into buffer i % NBUF
         const int buf = i % NBUF;
@@ -134,7 +144,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
                 v[b * R0 + r] = MODE == SM_INV ? cconj(e) : e;
             }
         __syncthreads();  // all stage-0 reads before the tile is reused for exchanges
-        rfft_plan<T, N, E, R0, R1, R2, false>(v, q, a.stw, a.stwl, x);
+        rfft_plan<T, N, E, R0, R1, R2, false>(v, q, twh, twl, x);
 
         int c1, c2;
         if (ypass) {
@@ -167,7 +177,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
                     const int pos = q + TL * b + r * (N / RL);
                     v[b * RL + r] = kinetic_apply(v[b * RL + r], dother, kda, kdaf, pos, a.tb.kscale);
                 }
-            rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+            rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
             if (valid) {
 #pragma unroll
                 for (int b = 0; b < E / R0; ++b)
@@ -224,6 +234,9 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
     constexpr int RL = kRev ? R0 : S::last;
     extern __shared__ __align__(1024) unsigned char smraw3[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smraw3 + (size_t)NBUF * BUF_BYTES);
+    using TW = TwStage<T, R0, R1, R2>;
+    cx<T>* twh = reinterpret_cast<cx<T>*>(smraw3 + pipe_tw_offset((size_t)NBUF * BUF_BYTES, NBUF));
+    const cx<T>* twl = TW::lo_of(twh);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int lw = lane / TL, q = lane % TL;
     const int nmine = blockIdx.x < (unsigned)pa.ntiles ? (pa.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -232,6 +245,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
         for (int b = 0; b < NBUF; ++b) mbar_init(smem_u32(&bars[b]), 1);
         fence_mbar_init();
     }
+    if (nmine > 0) TW::load(twh, f.args(blockIdx.x).stw, f.args(blockIdx.x).stwl);
     __syncthreads();
     auto issue = [&](int i) {
         const int buf = i % NBUF;
@@ -295,7 +309,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                 v[b * RF + r] = kConjIn ? cconj(e) : e;
             }
         __syncwarp();  // the line is reused for exchanges: all stage-0 reads first
-        rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, a.stw, a.stwl, x);
+        rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, twh, twl, x);
 
         if constexpr (MODE == XM_FWD || MODE == XM_START || MODE == XM_END) {
             if (valid) {
@@ -332,7 +346,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                     }
                     v[b * RL + r] = e;
                 }
-            rfft_plan<T, N, E, R0, R1, R2, true>(v, q, a.stw, a.stwl, x);
+            rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
             if (valid) {
 #pragma unroll
                 for (int b = 0; b < E / R0; ++b)

@@ -18,6 +18,8 @@ struct PlanEntry {
     int n = 0, e = 0, r0 = 1, r1 = 1, r2 = 1;
     int ls = 0;             // lines per strided-pass CTA
     int xw = 4;             // warps per contiguous-pass CTA
+    size_t twb = 0;         // bytes of the shared-memory stage-twiddle copy (persistent kernels)
+    size_t xbsm = 0;        // dynamic shared memory of the batched register-path x pass
     PassKernel<T> xk[7];    // by XMode
     PassKernel<T> sk[kSModes];  // by SModeK
     // pipelined variants; the solver picks one per axis (default 0, or autotuned)
@@ -67,6 +69,8 @@ PlanEntry<T> make_plan_entry() {
     p.r2 = R2;
     p.ls = LS;
     p.xw = XShape<T, N, E>::NW;
+    p.twb = TwStage<T, R0, R1, R2>::bytes;
+    p.xbsm = xbatch_smem<T, N, E, R0, R1, R2>();
     p.xk[XM_FWD] = xpass2_kernel<T, XM_FWD, N, E, R0, R1, R2>;
     p.xk[XM_INV] = xpass2_kernel<T, XM_INV, N, E, R0, R1, R2>;
     p.xk[XM_START] = xpass2_kernel<T, XM_START, N, E, R0, R1, R2>;
@@ -91,14 +95,16 @@ PlanEntry<T> make_plan_entry() {
     p.sb[SM_INV] = sbatch_kernel<T, SM_INV, N, E, R0, R1, R2, LS>;
     p.sb[SM_FUSED] = sbatch_kernel<T, SM_FUSED, N, E, R0, R1, R2, LS>;
     for (int m = 0; m < 7; ++m)
-        if (p.xb[m])
-            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&p.xb_bps[m], p.xb[m], p.xw * 32, 0,
+        if (p.xb[m]) {
+            allow_smem(p.xb[m], (int)p.xbsm);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&p.xb_bps[m], p.xb[m], p.xw * 32, p.xbsm,
                                                                   cudaOccupancyDefault);
+        }
     for (int m = 0; m < kSModes; ++m)
         if (p.sb[m]) {
-            allow_smem(p.sb[m], smem);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&p.sb_bps[m], p.sb[m], LS * (N / E), smem,
-                                                                  cudaOccupancyDefault);
+            allow_smem(p.sb[m], smem + (int)p.twb);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&p.sb_bps[m], p.sb[m], LS * (N / E),
+                                                                  smem + p.twb, cudaOccupancyDefault);
         }
     cudaGetLastError();
     return p;
@@ -126,7 +132,7 @@ void add_x_variant(PlanEntry<T>& p) {
         v.kb[XM_END] = xbatch3_kernel<T, XM_END, N, E, R0, R1, R2, NW, NBUF, MINB>;
     }
     for (int m : {XM_FWD, XM_START, XM_MID, XM_END}) {
-        v.smem[m] = NBUF * (m != XM_FWD ? 2 * psi : psi) + NBUF * sizeof(uint64_t);
+        v.smem[m] = pipe_tw_offset(NBUF * (m != XM_FWD ? 2 * psi : psi), NBUF) + TwStage<T, R0, R1, R2>::bytes;
         allow_smem(v.k[m], (int)v.smem[m]);
         cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bps[m], v.k[m], NW * 32, v.smem[m],
                                                               cudaOccupancyDefault);
@@ -154,7 +160,7 @@ void add_s_variant(PlanEntry<T>& p) {
         v.kb[SM_INV] = sbatch3_kernel<T, SM_INV, N, E, R0, R1, R2, LS, NBUF, MINB>;
         v.kb[SM_FUSED] = sbatch3_kernel<T, SM_FUSED, N, E, R0, R1, R2, LS, NBUF, MINB>;
     }
-    v.smem = NBUF * (size_t)N * LS * sizeof(cx<T>) + NBUF * sizeof(uint64_t);
+    v.smem = pipe_tw_offset(NBUF * (size_t)N * LS * sizeof(cx<T>), NBUF) + TwStage<T, R0, R1, R2>::bytes;
     for (int m : {SM_FWD, SM_INV, SM_FUSED}) {
         allow_smem(v.k[m], (int)v.smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bps[m], v.k[m], LS * TL, v.smem,
