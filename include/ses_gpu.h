@@ -101,6 +101,19 @@ SES_API ses_status ses_device_count(int* out);
  * and mass = 1. */
 SES_API ses_status ses_gpu_create(const ses_grid_desc* grid, ses_precision prec, double dt, double mass,
                           const double* V, const double* psi0, ses_handle* out);
+/* ImaginaryTimePropagator3D(grid, V, dtau, mass) (core/src/imaginary_time.ixx:64-96) and the
+ * GPU relax path (solver/src/vk_engine.ixx:1047-1080): the same handle with the real weights
+ * exp(-V dtau/2) and exp(-k^2 dtau/(2m)) in place of the phase tables.  Step it with
+ * ses_gpu_relax; ses_gpu_observe gives <H>.  Lines above 4096 points are not supported. */
+SES_API ses_status ses_gpu_create_imag(const ses_grid_desc* grid, ses_precision prec, double dtau, double mass,
+                                       const double* V, const double* psi0, ses_handle* out);
+/* relax(Field3D&, nsteps) (imaginary_time.ixx:98-108): nsteps Strang steps of imaginary
+ * time, psi renormalised to sum |psi|^2 dV = 1 on the device every renorm_every steps
+ * (<= 0: every step, as the reference; the result differs only by rounding since the step
+ * is linear).  energy (nullable): -ln(norm^2) / (2 r dtau) over the last r steps before
+ * the final renormalisation, which converges to the ground-state energy; with energy
+ * NULL the call only queues the work. */
+SES_API ses_status ses_gpu_relax(ses_handle h, int nsteps, int renorm_every, double* energy);
 /* Engine::destroy (vk_engine.ixx) */
 SES_API ses_status ses_gpu_destroy(ses_handle h);
 /* Engine::set_potential (vk_engine.ixx): rebuild the potential phase table. */

@@ -54,6 +54,36 @@ __global__ void build_vtab_c64(const double* __restrict__ V, cx<float>* out, lon
     }
 }
 
+// Imaginary time (imaginary_time.ixx:71-95): real weights exp(-V dtau/2) and
+// exp(-k^2 dtau/(2m)) in the tables' formats -- complex128 (w, 0), complex64
+// the delta (w - 1, 0) from expm1, so small weights-minus-one stay accurate.
+__global__ void build_vtab_imag_c128(const double* __restrict__ V, cx<double>* out, long long N, double dtau) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = mk<double>(exp(theta_v(V[i], dtau)), 0.0);
+}
+
+__global__ void build_vtab_imag_c64(const double* __restrict__ V, cx<float>* out, long long N, double dtau) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = mk<float>((float)expm1(theta_v(V[i], dtau)), 0.0f);
+}
+
+__global__ void build_axis_tables_imag(int n, double dtau, double mass, const double* kv, cx<double>* kd) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) kd[j] = mk<double>(expm1(theta_k(__dmul_rn(kv[j], kv[j]), mass, dtau)), 0.0);
+}
+
+// psi *= 1 / sqrt(sum |psi|^2 dV), the sum taken from sums[0] on the device;
+// sums[0] is kept for the energy estimate.
+template <typename T>
+__global__ void renormalize_kernel(cx<T>* psi, long long N, const double* __restrict__ sums, double dv) {
+    const double s = 1.0 / sqrt(sums[0] * dv);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x)
+        psi[i] = scale_d(psi[i], s);
+}
+
 // per-axis wavenumbers k_j = (2 pi / L) * (j if 2j < n else j - n)  (spectral.ixx:14-23)
 // and kinetic deltas cis(-k^2 dt/(2m)) - 1
 __global__ void build_axis_tables(double xmin, double xmax, int n, double dt, double mass,

@@ -264,6 +264,7 @@ struct ses_solver {
     // long 1D line (nx > 4096, ny = nz = 1) stored as n[0] x n[1] = N1 x N2 and
     // transformed in four steps; box[0..1] and N keep the physical line
     bool long1d = false;
+    bool imag = false;       // imaginary-time handle: real weight tables, no absorber
     void* kfull = nullptr;   // kinetic delta per stored k-space element
     void* tw4 = nullptr;     // W_N^{n1 k2} per element (complex64: hi part)
     void* tw4l = nullptr;    // complex64: lo part
@@ -687,6 +688,40 @@ ses_status enqueue_fft3(ses_solver* h, void* data, int inverse) {
     return pass_x<T>(h, data, data, p, s);
 }
 
+ObsArgs obs_args(const ses_solver* h, double xlo, double xhi);
+
+// Imaginary time: psi /= sqrt(sum |psi|^2 dV) on the device (the sum stays in dsums[0]).
+template <typename T>
+ses_status enqueue_renormalize(ses_solver* h) {
+    cudaStream_t s = h->stream;
+    const ObsArgs o = obs_args(h, -1e300, 1e300);
+    obs_real_kernel<T><<<kObsBlocks, 256, 0, s>>>(reinterpret_cast<const cx<T>*>(h->psi), h->V, o, h->partials);
+    finalize_kernel<<<1, 32, 0, s>>>(h->partials, kObsBlocks, kRedR, h->dsums);
+    const double dv = o.hx * o.hy * o.hz;
+    const unsigned gb = (unsigned)std::min<long long>((h->N + 255) / 256, 148 * 16);
+    renormalize_kernel<T><<<gb, 256, 0, s>>>(reinterpret_cast<cx<T>*>(h->psi), h->N, h->dsums, dv);
+    SES_CU(cudaGetLastError());
+    return SES_OK;
+}
+
+ObsArgs obs_args(const ses_solver* h, double xlo, double xhi) {
+    ObsArgs o{};
+    o.N = h->N;
+    o.nx = phys_n(h, 0);
+    o.ny = phys_n(h, 1);
+    o.fnx = make_fastdiv((uint32_t)o.nx);
+    o.fny = make_fastdiv((uint32_t)o.ny);
+    o.x0 = h->box[0];
+    o.hx = (h->box[1] - h->box[0]) / phys_n(h, 0);
+    o.y0 = h->box[2];
+    o.hy = (h->box[3] - h->box[2]) / phys_n(h, 1);
+    o.z0 = h->box[4];
+    o.hz = (h->box[5] - h->box[4]) / phys_n(h, 2);
+    o.xlo = xlo;
+    o.xhi = xhi;
+    return o;
+}
+
 template <typename T>
 ses_status enqueue_observe(ses_solver* h, double xlo, double xhi) {
     cudaStream_t s = h->stream;
@@ -1008,6 +1043,14 @@ ses_status build_tables(ses_solver* h) {
     const long long N = h->N;
     const int tb = 256;
     const unsigned gb = (unsigned)std::min<long long>((N + tb - 1) / tb, 148 * 32);
+    if (h->imag) {
+        if (h->prec == SES_C128)
+            build_vtab_imag_c128<<<gb, tb, 0, h->stream>>>(h->V, reinterpret_cast<cx<double>*>(h->vtab), N, h->dt);
+        else
+            build_vtab_imag_c64<<<gb, tb, 0, h->stream>>>(h->V, reinterpret_cast<cx<float>*>(h->vtab), N, h->dt);
+        SES_CU(cudaGetLastError());
+        return SES_OK;
+    }
     if (h->prec == SES_C128)
         build_vtab_c128<<<gb, tb, 0, h->stream>>>(h->V, reinterpret_cast<cx<double>*>(h->vtab), N,
                                                    h->dt);
@@ -1151,7 +1194,8 @@ void build_tmaps(ses_solver* h, int buf, void* base) {
 }
 
 ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt, double mass,
-                       const double* V, const double* psi0, bool with_tables, ses_handle* out) {
+                       const double* V, const double* psi0, bool with_tables, ses_handle* out,
+                       bool imag = false) {
     if (!grid || !out) return fail(SES_EINVAL, "null grid or output pointer");
     *out = nullptr;
     if (prec != SES_C128 && prec != SES_C64) return fail(SES_EINVAL, "unknown precision");
@@ -1186,6 +1230,8 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
                 break;
             }
         }
+        if (imag)
+            return fail(SES_EINVAL, "imaginary time supports lines up to 4096 points");
         if (!long_n1)
             return fail(SES_EINVAL, "1D line of " + std::to_string(ax[0].n) +
                                         " points: lines above 4096 need N = N1 x N2 with both factors in "
@@ -1199,6 +1245,7 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
     h->dt = dt;
     h->mass = mass;
     h->with_tables = with_tables;
+    h->imag = imag;
     for (int a = 0; a < 3; ++a) {
         h->n[a] = ax[a].n;
         h->box[2 * a] = ax[a].xmin;
@@ -1262,6 +1309,7 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
         build_axis_tables<<<gb, 256, 0, h->stream>>>(h->box[2 * a], h->box[2 * a + 1], n,
                                                      with_tables ? dt : 0.0,
                                                      with_tables ? mass : 1.0, h->kv[a], h->kd[a]);
+        if (imag) build_axis_tables_imag<<<gb, 256, 0, h->stream>>>(n, dt, mass, h->kv[a], h->kd[a]);
         if ((st = dalloc(h, (void**)&h->kdf[a], (size_t)n * sizeof(cx<float>))) != SES_OK) return bail(st);
         convert_kernel<double, float><<<gb, 256, 0, h->stream>>>(h->kd[a], h->kdf[a], n);
     }
@@ -1908,6 +1956,33 @@ ses_status ses_gpu_create(const ses_grid_desc* grid, ses_precision prec, double 
     return create_impl(grid, prec, dt, mass, V, psi0, true, out);
 }
 
+ses_status ses_gpu_create_imag(const ses_grid_desc* grid, ses_precision prec, double dtau, double mass,
+                               const double* V, const double* psi0, ses_handle* out) {
+    if (!(dtau > 0.0)) return fail(SES_EINVAL, "dtau must be > 0");
+    return create_impl(grid, prec, dtau, mass, V, psi0, true, out, true);
+}
+
+ses_status ses_gpu_relax(ses_handle h, int nsteps, int renorm_every, double* energy) {
+    SES_TRY(check_handle(h));
+    if (!h->imag) return fail(SES_EINVAL, "handle was not created for imaginary time (ses_gpu_create_imag)");
+    if (nsteps < 1) return fail(SES_EINVAL, "nsteps must be >= 1");
+    const int R = renorm_every > 0 ? renorm_every : 1;
+    int done = 0, last = 1;
+    while (done < nsteps) {
+        last = std::min(R, nsteps - done);
+        SES_TRY(h->prec == SES_C128 ? enqueue_steps<double>(h, last, false) : enqueue_steps<float>(h, last, false));
+        SES_TRY(h->prec == SES_C128 ? enqueue_renormalize<double>(h) : enqueue_renormalize<float>(h));
+        done += last;
+    }
+    if (!energy) return SES_OK;
+    SES_CU(cudaMemcpyAsync(h->hsums, h->dsums, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    SES_TRY(wait_bounded(h, 0));
+    const ObsArgs o = obs_args(h, 0.0, 0.0);
+    const double n2 = h->hsums[0] * o.hx * o.hy * o.hz;  // norm^2 after the last `last` steps
+    *energy = -std::log(n2) / (2.0 * last * h->dt);
+    return SES_OK;
+}
+
 ses_status ses_gpu_destroy(ses_handle h) {
     SES_TRY(check_handle(h));
     if (h->batch) SES_TRY(batch_remove_impl(h->batch, h));
@@ -2016,6 +2091,7 @@ ses_status ses_gpu_fft3(ses_handle h, int direction) {
 
 ses_status ses_gpu_tables(ses_handle h, double* half_v, double* kin) {
     SES_TRY(check_handle(h));
+    if (h->imag) return fail(SES_EINVAL, "imaginary-time handle: its tables are real weights, not phases");
     if (!h->with_tables) return fail(SES_EINVAL, "handle has no phase tables");
     if (!half_v && !kin) return SES_OK;
     void *dh = nullptr, *dk = nullptr;

@@ -229,12 +229,17 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
             cp_async_commit();
         }
     }
-    // potential / mask at element pos of this line; the table entry from vrow when prefetched
+    // potential / mask at element pos of this line; the table entry from vrow when
+    // prefetched, the separable mask as mx[pos] times the line's my[j] mz[k]
+    const double* mfull = a.tb.maskfull;
+    const double* mx = a.tb.mask1[0];
+    const double myz = (!mfull && mx) ? a.tb.mask1[1][jy] * a.tb.mask1[2][kz] : 1.0;
     auto diag = [&](cx<T> e, int kind, int msk, int pos) {
         const long long f = mc * N + pos;
         if (vrow) {
             const cx<T> tab = kind != DG_NONE ? vrow[pos] : e;
-            return apply_diag_tv(e, kind, tab, msk, msk ? maskval<T>(a.tb, f, pos, jy, kz) : 1.0);
+            const double mv = !msk ? 1.0 : (mfull ? mfull[f] : mx[pos] * myz);
+            return apply_diag_tv(e, kind, tab, msk, mv);
         }
         return apply_diag(e, kind, msk, f, pos, jy, kz, a.tb);
     };
