@@ -132,6 +132,13 @@ SES_API ses_status ses_gpu_set_absorber_separable(ses_handle h, const double* mx
  * are merged into full kicks, so psi is in real space only at batch ends.
  * Asynchronous: returns once the work is queued on the handle's stream. */
 SES_API ses_status ses_gpu_step(ses_handle h, int nsteps, int absorb);
+/* driven_step(psi, prop, DipoleDrive{axis, amplitude, omega}, t0, nsteps) (core/src/drive.ixx:50-65)
+ * and Engine::driven_step (solver/src/vk_engine.ixx:836-876): each step is
+ * kick(t) . Strang step . kick(t + dt), kick = psi * cis(-theta (axis . r)),
+ * theta = amplitude cos(omega t) dt/2, t = t0 + s dt; absorb as in ses_gpu_step.
+ * 2D and 3D grids.  The kick between two steps is applied as one phase. */
+SES_API ses_status ses_gpu_step_driven(ses_handle h, int nsteps, int absorb, const double* axis, double amplitude,
+                                       double omega, double t0);
 /* fft(Field3D&) / ifft(Field3D&) (core/src/fft.ixx:102-188) on the resident
  * psi: direction 0 = forward (unnormalised), 1 = inverse (1/N). */
 SES_API ses_status ses_gpu_fft3(ses_handle h, int direction);

@@ -43,7 +43,7 @@ LIB = OUT / "libsesref.so"
 # Reference core modules on the split-operator path (core/src/<m>.ixx).
 MODULES = [
     "grid", "vec", "parallel", "field", "spectral", "fft", "propagator",
-    "potential", "wavepacket", "observables", "imaginary_time",
+    "potential", "wavepacket", "observables", "imaginary_time", "drive",
 ]
 
 FLAGS = ["-std=c++20", "-O2", "-mavx2", "-mfma", "-ffp-contract=off",

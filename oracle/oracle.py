@@ -83,6 +83,9 @@ class Oracle:
         L.seso_step1d.restype = C.c_int
         L.seso_relax3d.argtypes = [_dp, _ip, _dp, C.c_double, C.c_double, _dp, C.c_int]
         L.seso_relax3d.restype = C.c_int
+        L.seso_driven_step3d.argtypes = [_dp, _ip, _dp, C.c_double, C.c_double, _dp, C.c_double, C.c_double,
+                                         C.c_double, _dp, C.c_int]
+        L.seso_driven_step3d.restype = C.c_int
         L.seso_harmonic3d.argtypes = [_dp, _ip, C.c_double, _dp, _dp]
         L.seso_soft_coulomb3d.argtypes = [_dp, _ip, C.c_double, C.c_double, _dp, _dp]
         L.seso_regularized_coulomb3d.argtypes = [_dp, _ip, C.c_double, _dp, _dp]
@@ -176,6 +179,17 @@ class Oracle:
         m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
         if self.lib.seso_step1d(xmin, xmax, n, _d(V), dt, _d(m), psi.ctypes.data_as(_dp),
                                 nsteps) != 0:
+            raise ValueError("unsupported grid")
+        return psi
+
+    def driven_step3d(self, box, n, V, dt, psi, nsteps, axis, amplitude, omega, t0=0.0, mass=1.0):
+        """drive.ixx:50-65: kick(t) . Strang step . kick(t + dt), no mask."""
+        b, nn = _box(box), _n(n)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        psi = np.array(psi, dtype=np.complex128, copy=True).reshape(-1)
+        ax = np.ascontiguousarray(axis, dtype=np.float64)
+        if self.lib.seso_driven_step3d(_d(b), _nptr(nn), _d(V), dt, mass, _d(ax), amplitude, omega, t0,
+                                       psi.ctypes.data_as(_dp), nsteps) != 0:
             raise ValueError("unsupported grid")
         return psi
 
@@ -366,6 +380,8 @@ class Reference:
                                                     C.c_double, C.c_double]
         L.sesref_probability_in_range1d.restype = C.c_double
         L.sesref_relax3d.argtypes = [_dp, _ip, _dp, C.c_double, C.c_double, _dp, C.c_int]
+        L.sesref_driven_step3d.argtypes = [C.c_void_p, C.c_void_p, _dp, C.c_double, C.c_double, C.c_double,
+                                           C.c_int]
 
     def workers(self) -> int:
         return self.lib.sesref_workers()
@@ -528,6 +544,10 @@ class RefSplit3D:
     def step(self, nsteps, mask=None):
         m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
         self.ref.lib.sesref_split3d_step(self.h, self.f, nsteps, _d(m))
+
+    def driven_step(self, nsteps, axis, amplitude, omega, t0=0.0):
+        ax = np.ascontiguousarray(axis, dtype=np.float64)
+        self.ref.lib.sesref_driven_step3d(self.h, self.f, _d(ax), amplitude, omega, t0, nsteps)
 
     def norm(self):
         return self.ref.lib.sesref_norm3d(self.f)

@@ -23,6 +23,7 @@
 #include "wavepacket.hpp"
 #include "observables.hpp"
 #include "imaginary_time.hpp"
+#include "drive.hpp"
 
 namespace {
 
@@ -187,6 +188,14 @@ void sesref_split3d_step(void* h, void* f, int nsteps, const double* mask) {
             a[static_cast<std::size_t>(i)] *= mask[i];
         });
     }
+}
+
+// ses::driven_step (drive.ixx:50-65) on the resident field.
+void sesref_driven_step3d(void* h, void* f, const double* axis, double amplitude, double omega, double t0,
+                          int nsteps) {
+    const auto* p = static_cast<Prop3*>(h);
+    ses::DipoleDrive d{ses::Vec3d{axis[0], axis[1], axis[2]}, amplitude, omega};
+    ses::driven_step(*static_cast<ses::Field3D*>(f), p->op, d, t0, nsteps);
 }
 
 double sesref_norm3d(void* f) { return ses::norm_sq(*static_cast<ses::Field3D*>(f)); }

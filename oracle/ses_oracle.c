@@ -322,6 +322,48 @@ int seso_step3d(const double* box, const int* n, const double* V, double dt, dou
     return 0;
 }
 
+/* Dipole-driven Strang steps (core/src/drive.ixx:25-65): kick(t) . step . kick(t + dt),
+ * kick = psi * cis(-theta u), theta = amplitude cos(omega t) dt/2, u = axis . r. */
+static void dipole_halfkick(cplx* a, const double* box, const int* n, const double* axis, double amplitude,
+                            double omega, double t, double dt) {
+    const double theta = amplitude * cos(omega * t) * 0.5 * dt;
+    for (int k = 0; k < n[2]; ++k)
+        for (int j = 0; j < n[1]; ++j)
+            for (int i = 0; i < n[0]; ++i) {
+                const double u = axis[0] * coord(box[0], box[1], n[0], i) + axis[1] * coord(box[2], box[3], n[1], j) +
+                                 axis[2] * coord(box[4], box[5], n[2], k);
+                const double ang = -theta * u;
+                const cplx c = {cos(ang), sin(ang)};
+                const size_t f = flat(n, i, j, k);
+                a[f] = cmul(a[f], c);
+            }
+}
+
+int seso_driven_step3d(const double* box, const int* n, const double* V, double dt, double mass,
+                       const double* axis, double amplitude, double omega, double t0, double* psi,
+                       int nsteps) {
+    for (int ax = 0; ax < 3; ++ax)
+        if (seso_supported_length((size_t)n[ax]) != 0) return -1;
+    const size_t N = total(n);
+    cplx* half = (cplx*)malloc(N * sizeof(cplx));
+    cplx* kin = (cplx*)malloc(N * sizeof(cplx));
+    seso_tables3d(box, n, V, dt, mass, (double*)half, (double*)kin);
+    cplx* a = (cplx*)psi;
+    for (int s = 0; s < nsteps; ++s) {
+        const double t = t0 + s * dt;
+        dipole_halfkick(a, box, n, axis, amplitude, omega, t, dt);
+        apply_phase(a, half, N);
+        seso_fft3d(psi, n);
+        apply_phase(a, kin, N);
+        seso_ifft3d(psi, n);
+        apply_phase(a, half, N);
+        dipole_halfkick(a, box, n, axis, amplitude, omega, t + dt, dt);
+    }
+    free(half);
+    free(kin);
+    return 0;
+}
+
 int seso_step1d(double xmin, double xmax, int n, const double* V, double dt, const double* mask,
                 double* psi, int nsteps) {
     if (seso_supported_length((size_t)n) != 0) return -1;

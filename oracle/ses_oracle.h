@@ -45,6 +45,10 @@ int seso_step3d(const double* box, const int* n, const double* V, double dt, dou
                 const double* mask, double* psi, int nsteps);
 int seso_step1d(double xmin, double xmax, int n, const double* V, double dt, const double* mask,
                 double* psi, int nsteps);
+/* dipole-driven steps kick(t) . step . kick(t + dt) (drive.ixx:25-65), no mask */
+int seso_driven_step3d(const double* box, const int* n, const double* V, double dt, double mass,
+                       const double* axis, double amplitude, double omega, double t0, double* psi,
+                       int nsteps);
 /* imaginary-time relaxation with renormalisation (imaginary_time.ixx:64-144) */
 int seso_relax3d(const double* box, const int* n, const double* V, double dtau, double mass,
                  double* psi, int nsteps);

@@ -28,6 +28,7 @@ EXPORTS = [
     "ses_batch_profile", "ses_batch_autotune", "ses_batch_info",
     "ses_serve_open", "ses_serve_submit", "ses_serve_poll", "ses_serve_result", "ses_serve_cancel",
     "ses_serve_wait_idle", "ses_serve_stats", "ses_serve_close", "ses_gpu_create_imag", "ses_gpu_relax",
+    "ses_gpu_step_driven",
 ]
 
 
@@ -102,6 +103,7 @@ def _load() -> C.CDLL:
         "ses_gpu_create_imag": ([C.POINTER(GridDesc), C.c_int, C.c_double, C.c_double, dp, dp,
                                  C.POINTER(hp)], st),
         "ses_gpu_relax": ([hp, C.c_int, C.c_int, dp], st),
+        "ses_gpu_step_driven": ([hp, C.c_int, C.c_int, dp, C.c_double, C.c_double, C.c_double], st),
         "ses_gpu_set_potential": ([hp, dp], st),
         "ses_gpu_set_absorber": ([hp, dp], st),
         "ses_gpu_set_absorber_separable": ([hp, dp, dp, dp], st),

@@ -249,6 +249,14 @@ class SplitOperator3D:
     def advance(self, nsteps: int, absorb: bool = False) -> None:
         check(lib.ses_gpu_step(self._h, int(nsteps), 1 if absorb else 0))
 
+    def advance_driven(self, nsteps: int, axis, amplitude: float, omega: float, t0: float = 0.0,
+                       absorb: bool = False) -> None:
+        """Dipole-driven steps on the resident psi (drive.ixx:50-65): each step is
+        kick(t) . step . kick(t + dt), kick phase amplitude cos(omega t) dt/2 (axis . r)."""
+        ax = np.ascontiguousarray(np.asarray(axis, dtype=np.float64).reshape(3))
+        check(lib.ses_gpu_step_driven(self._h, int(nsteps), 1 if absorb else 0, ax.ctypes.data_as(_dp),
+                                      float(amplitude), float(omega), float(t0)))
+
     def set_absorber(self, mask) -> None:
         if mask is None:
             check(lib.ses_gpu_set_absorber(self._h, None))
@@ -336,6 +344,21 @@ class SplitOperator3D:
 
     def __exit__(self, *exc):
         self.close()
+
+
+@dataclass
+class DipoleDrive:
+    """Polarization axis (need not be unit: scales E0), amplitude E0, angular frequency (drive.ixx:19-23)."""
+    axis: tuple
+    amplitude: float
+    omega: float
+
+
+def driven_step(psi: Field3D, prop: "SplitOperator3D", d: DipoleDrive, t0: float, nsteps: int) -> None:
+    """ses::driven_step (drive.ixx:50-65) on a caller-owned field: upload, nsteps driven steps, readback."""
+    prop.upload_state(psi.data)
+    prop.advance_driven(nsteps, d.axis, d.amplitude, d.omega, t0)
+    prop.readback(out=psi.data)
 
 
 class ImaginaryTimePropagator3D(SplitOperator3D):

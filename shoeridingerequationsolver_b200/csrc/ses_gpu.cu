@@ -485,6 +485,8 @@ struct XProg {
     int d_load = DG_NONE, d_mid = DG_NONE, d_store = DG_NONE;
     int m_load = 0, m_mid = 0, m_store = 0;
     double out_scale = 1.0;
+    double kick = 0.0;                  // dipole kick theta at this pass's potential site
+    const double* kick_axis = nullptr;  // polarization (3 doubles)
 };
 
 template <typename T>
@@ -497,6 +499,14 @@ ses_status pass_x(const ses_solver* h, const void* src, void* dst, const XProg& 
     a.m_mid = p.m_mid;
     a.m_store = p.m_store;
     a.out_scale = p.out_scale;
+    if (p.kick != 0.0) {
+        a.tb.kick = p.kick;
+        for (int q = 0; q < 3; ++q) {
+            a.tb.kax[q] = p.kick_axis[q];
+            a.tb.korg[q] = h->box[2 * q];
+            a.tb.kh[q] = (h->box[2 * q + 1] - h->box[2 * q]) / phys_n(h, q);
+        }
+    }
     return launch<T>(h, 0, p.mode, a, s);
 }
 
@@ -666,6 +676,44 @@ ses_status enqueue_steps(ses_solver* h, int S, bool mask) {
     end.mode = XM_END;
     end.d_store = DG_HALF;
     end.m_store = mask;
+    return pass_x<T>(h, h->psi, h->psi, end, s);
+}
+
+// Dipole-driven steps (drive.ixx:50-65): kick(t) . step . kick(t + dt) with
+// kick theta(t) = amplitude cos(omega t) dt/2; the kicks are diagonal like the
+// potential, so they ride on the x passes that apply it (the kick ending step s
+// and the one starting step s + 1 as one phase).  Direct launches: the phases
+// change every step.
+template <typename T>
+ses_status enqueue_driven(ses_solver* h, int S, bool mask, const double* axis, double amp, double omega,
+                          double t0) {
+    cudaStream_t s = h->stream;
+    const double dt = h->dt;
+    auto theta = [&](double t) { return amp * std::cos(omega * t) * 0.5 * dt; };
+    XProg start;
+    start.mode = XM_START;
+    start.d_load = DG_HALF;
+    start.kick = theta(t0);
+    start.kick_axis = axis;
+    SES_TRY(pass_x<T>(h, h->psi, h->psi, start, s));
+    SES_TRY(mid_axes<T>(h, s));
+    for (int k = 1; k < S; ++k) {
+        const double t_prev = t0 + (k - 1) * dt, t = t0 + k * dt;
+        XProg mid;
+        mid.mode = XM_MID;
+        mid.d_mid = DG_FULL;
+        mid.m_mid = mask;
+        mid.kick = theta(t_prev + dt) + theta(t);
+        mid.kick_axis = axis;
+        SES_TRY(pass_x<T>(h, h->psi, h->psi, mid, s));
+        SES_TRY(mid_axes<T>(h, s));
+    }
+    XProg end;
+    end.mode = XM_END;
+    end.d_store = DG_HALF;
+    end.m_store = mask;
+    end.kick = theta(t0 + (S - 1) * dt + dt);
+    end.kick_axis = axis;
     return pass_x<T>(h, h->psi, h->psi, end, s);
 }
 
@@ -2077,6 +2125,19 @@ ses_status ses_gpu_step(ses_handle h, int nsteps, int absorb) {
     const bool mask = absorb != 0 && h->has_mask;
     return h->prec == SES_C128 ? enqueue_steps<double>(h, nsteps, mask)
                                : enqueue_steps<float>(h, nsteps, mask);
+}
+
+ses_status ses_gpu_step_driven(ses_handle h, int nsteps, int absorb, const double* axis, double amplitude,
+                               double omega, double t0) {
+    SES_TRY(check_handle(h));
+    if (!h->with_tables || h->imag) return fail(SES_EINVAL, "handle has no real-time phase tables");
+    if (!axis) return fail(SES_EINVAL, "null polarization axis");
+    if (h->last_axis == 0 || h->long1d) return fail(SES_EINVAL, "the dipole drive steps 2D and 3D grids");
+    if (nsteps < 0) return fail(SES_EINVAL, "nsteps must be >= 0");
+    if (nsteps == 0) return SES_OK;
+    const bool mask = absorb != 0 && h->has_mask;
+    return h->prec == SES_C128 ? enqueue_driven<double>(h, nsteps, mask, axis, amplitude, omega, t0)
+                               : enqueue_driven<float>(h, nsteps, mask, axis, amplitude, omega, t0);
 }
 
 ses_status ses_gpu_fft3(ses_handle h, int direction) {

@@ -44,6 +44,10 @@ struct Tables {
     const void* tw4;           // W_N^{n1 k2} per element (cx<T>; complex64: FP32-rounded)
     const void* tw4l;          // complex64: FP32 remainder of tw4
     int long_n2;               // N2: stored element (k1, k2) is frequency k2 + N2 k1
+    // dipole drive (drive.ixx:25-40): psi *= cis(-kick u), u = axis . r at cell (i, j, k),
+    // r = origin + index * spacing; kick = 0 off
+    double kick;
+    double kax[3], korg[3], kh[3];
 };
 
 // complex64 phase multiplies in FP32 on the delta form: psi + psi*d, d = factor - 1.
@@ -89,12 +93,31 @@ __device__ __forceinline__ double maskval(const Tables& tb, long long f, int i, 
 template <typename T>
 __device__ __forceinline__ cx<T> apply_diag_tv(cx<T> v, int kind, cx<T> tab, int use_mask, double m);
 
-// psi * (potential phase) * (mask) at flat index f, coordinates (i, j, k).
+// Dipole kick of cell (i, j, k): psi * cis(-kick (ax x + ay y + az z)), the phase in FP64;
+// complex64 multiplies in FP32 on the delta form.
+template <typename T>
+__device__ __forceinline__ cx<T> kick_mul(cx<T> v, const Tables& tb, int i, int j, int k) {
+    if (tb.kick == 0.0) return v;
+    const double u = tb.kax[0] * (tb.korg[0] + i * tb.kh[0]) + tb.kax[1] * (tb.korg[1] + j * tb.kh[1]) +
+                     tb.kax[2] * (tb.korg[2] + k * tb.kh[2]);
+    const double ang = -tb.kick * u;
+    if constexpr (sizeof(T) == 4) {
+        double s2, c2;
+        sincos(0.5 * ang, &s2, &c2);
+        return add_mul(v, mk<float>((float)(-2.0 * s2 * s2), (float)(2.0 * s2 * c2)));
+    } else {
+        double s, c;
+        sincos(ang, &s, &c);
+        return v * mk<double>(c, s);
+    }
+}
+
+// psi * (potential phase) * (mask) * (dipole kick) at flat index f, coordinates (i, j, k).
 template <typename T>
 __device__ __forceinline__ cx<T> apply_diag(cx<T> v, int kind, int use_mask, long long f, int i, int j,
                                             int k, const Tables& tb) {
     const cx<T> tab = kind != DG_NONE ? reinterpret_cast<const cx<T>*>(tb.vtab)[f] : v;
-    return apply_diag_tv(v, kind, tab, use_mask, use_mask ? maskval<T>(tb, f, i, j, k) : 1.0);
+    return kick_mul(apply_diag_tv(v, kind, tab, use_mask, use_mask ? maskval<T>(tb, f, i, j, k) : 1.0), tb, i, j, k);
 }
 
 // Same as apply_diag with the potential-table entry and mask value supplied

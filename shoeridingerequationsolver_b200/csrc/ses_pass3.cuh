@@ -303,8 +303,8 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                 cx<T> e = line[pos];
                 if constexpr (MODE == XM_START || MODE == XM_1D) {
                     if (a.d_load != DG_NONE || a.m_load)
-                        e = apply_diag_tv(e, a.d_load, tline[pos], a.m_load,
-                                          a.m_load ? mval(pos) : 1.0);
+                        e = kick_mul(apply_diag_tv(e, a.d_load, tline[pos], a.m_load, a.m_load ? mval(pos) : 1.0),
+                                     a.tb, pos, jy, kz);
                 }
                 v[b * RF + r] = kConjIn ? cconj(e) : e;
             }
@@ -322,8 +322,9 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                         if constexpr (MODE == XM_END) {
                             e = cconj(e);
                             if (a.d_store != DG_NONE || a.m_store)
-                                e = apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
-                                                  a.m_store ? mval(pos) : 1.0);
+                                e = kick_mul(apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
+                                                           a.m_store ? mval(pos) : 1.0),
+                                             a.tb, pos, jy, kz);
                         }
                         dst[pos] = e;
                     }
@@ -339,8 +340,8 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                     if constexpr (MODE == XM_MID) {
                         e = cconj(e);
                         if (a.d_mid != DG_NONE || a.m_mid)
-                            e = apply_diag_tv(e, a.d_mid, tline[pos], a.m_mid,
-                                              a.m_mid ? mval(pos) : 1.0);
+                            e = kick_mul(apply_diag_tv(e, a.d_mid, tline[pos], a.m_mid, a.m_mid ? mval(pos) : 1.0),
+                                         a.tb, pos, jy, kz);
                     } else {
                         e = kinetic_conj(e, dmul1(dyz, a.tb.kd[0][pos]), a.tb.kscale);
                     }
@@ -357,8 +358,9 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                         if constexpr (MODE == XM_1D) {
                             e = cconj(e);
                             if (a.d_store != DG_NONE || a.m_store)
-                                e = apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
-                                                  a.m_store ? mval(pos) : 1.0);
+                                e = kick_mul(apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
+                                                           a.m_store ? mval(pos) : 1.0),
+                                             a.tb, pos, jy, kz);
                         }
                         dst[pos] = e;
                     }

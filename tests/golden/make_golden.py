@@ -105,6 +105,16 @@ def main() -> int:
     out["relax_16cube_V"], out["relax_16cube_psi0"] = vi, pi0
     out["relax_16cube_psi50"] = ref.relax3d(boxi, ni, vi, 0.01, pi0, 50)
 
+    # dipole drive (drive.ixx:25-65): kick(t) . step . kick(t + dt), 16 x 8 x 8 harmonic
+    boxd, nd = (-6.0, 6.0, -5.0, 5.0, -4.0, 4.0), (16, 8, 8)
+    vd = ref.harmonic3d(boxd, nd, 1.0)
+    pd = ref.gaussian3d(boxd, nd, (0.5, 0.0, 0.0), (1.0, 1.0, 1.0), (0.3, 0.0, 0.0))
+    sd = ref.split3d(boxd, nd, vd, 0.05)
+    sd.set_psi(pd)
+    sd.driven_step(7, (0.6, 0.0, 0.8), 0.3, 1.1, 0.2)
+    out["drive_16x8x8_psi7"] = sd.get_psi()
+    sd.close()
+
     np.savez_compressed(HERE / "reference_core.npz", **out)
     size = (HERE / "reference_core.npz").stat().st_size
     print(f"wrote {len(out)} arrays, {size / 1024:.0f} KiB")

@@ -1,0 +1,31 @@
+"""Dipole-driven steps (ses_gpu_step_driven) against the FP64 oracle's restatement
+of the reference ses::driven_step (core/src/drive.ixx:50-65), which is pinned bit
+for bit to the reference library (tests/test_oracle_pins.py)."""
+
+import numpy as np
+import pytest
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,prec,tol", [((32, 32, 32), "c128", 1e-11), ((48, 32, 16), "c128", 1e-11),
+                                           ((64, 64, 1), "c128", 1e-11), ((32, 32, 32), "c64", 1e-5)])
+def test_driven_steps_match_oracle(ses, oracle, dims, prec, tol):
+    box = (-8.0, 8.0, -7.0, 7.0, -6.0, 6.0) if dims[2] > 1 else (-8.0, 8.0, -7.0, 7.0, 0.0, 1.0)
+    V = oracle.harmonic3d(box, dims, 0.8)
+    psi = oracle.gaussian3d(box, dims, (1.0, -0.5, 0.0), (1.2, 1.0, 1.1 if dims[2] > 1 else 1.0),
+                            (0.4, 0.0, 0.0))
+    g = ses.Grid3D(*[ses.Grid1D(box[2 * a], box[2 * a + 1], dims[a]) for a in range(3)])
+    op = ses.SplitOperator3D(g, V, 0.02, precision=prec, psi0=psi)
+    drive = ses.DipoleDrive((0.6, 0.8, 0.0), 0.5, 1.3)
+    f = ses.Field3D(g, psi)
+    ses.driven_step(f, op, drive, 0.1, 12)
+    want = oracle.driven_step3d(box, dims, V, 0.02, psi, 12, drive.axis, 0.5, 1.3, 0.1)
+    assert rel(f.data, want) <= tol
+    # the drive moves the packet: different from the undriven step
+    plain = oracle.step3d(box, dims, V, 0.02, psi, 12)
+    assert rel(want, plain) > 1e-3
+    op.close()

@@ -82,6 +82,14 @@ def test_line_and_relax_golden_bitwise(oracle):
     assert same(oracle.relax3d(box, n, V, 0.01, p, 50), GOLD["relax_16cube_psi50"])
 
 
+def test_dipole_drive_golden_bitwise(oracle):
+    box, n = (-6.0, 6.0, -5.0, 5.0, -4.0, 4.0), (16, 8, 8)
+    V = oracle.harmonic3d(box, n, 1.0)
+    p = oracle.gaussian3d(box, n, (0.5, 0.0, 0.0), (1.0, 1.0, 1.0), (0.3, 0.0, 0.0))
+    got = oracle.driven_step3d(box, n, V, 0.05, p, 7, (0.6, 0.0, 0.8), 0.3, 1.1, 0.2)
+    assert same(got, GOLD["drive_16x8x8_psi7"])
+
+
 def test_builders_golden_bitwise(oracle):
     box16, n16 = (-8.0, 8.0) * 3, (16, 16, 16)
     assert same(oracle.regularized_coulomb3d(box16, n16, 1.0), GOLD["coulomb_16cube_h1"])
