@@ -157,6 +157,18 @@ SES_API ses_status ses_gpu_observe(ses_handle h, double xlo, double xhi, ses_obs
  * rounds on upload and widens on readback).  Both block until done. */
 SES_API ses_status ses_gpu_read_psi(ses_handle h, double* psi_out);
 SES_API ses_status ses_gpu_write_psi(ses_handle h, const double* psi_in);
+/* psi snapshot wire format (the readback / upload_state layout of Engine,
+ * solver/src/vk_engine.ixx:2136-2155, 2413-2421, with a header): 128-byte header
+ * {"SESPSI1", precision, n[3], box[6], dt, mass, steps} then psi in the handle's own
+ * precision, interleaved float (SES_C64) or double (SES_C128) pairs, x fastest, no
+ * conversion.  For checkpoints and preemption.  Snapshot with out = NULL only
+ * reports the size; restore checks precision and grid.  Both block. */
+SES_API ses_status ses_gpu_snapshot(ses_handle h, int64_t steps, void* out, size_t cap, size_t* bytes);
+SES_API ses_status ses_gpu_restore(ses_handle h, const void* snap, size_t bytes, int64_t* steps);
+/* |psi|^2 (FP32) of the plane `index` along `axis` (0 x, 1 y, 2 z), the other two
+ * axes in order (lower axis fastest): nx*ny floats for axis 2, and so on.  For
+ * streaming density slices.  Blocks. */
+SES_API ses_status ses_gpu_density_slice(ses_handle h, int axis, int index, float* out);
 /* Wait for the handle's queued work; the wait is bounded by timeout_ms
  * (<= 0: 10 s, the reference's fence limit vk_compute.ixx:297-327) and
  * returns SES_ETIMEDOUT when it expires. */

@@ -28,7 +28,7 @@ EXPORTS = [
     "ses_batch_profile", "ses_batch_autotune", "ses_batch_info",
     "ses_serve_open", "ses_serve_submit", "ses_serve_poll", "ses_serve_result", "ses_serve_cancel",
     "ses_serve_wait_idle", "ses_serve_stats", "ses_serve_close", "ses_gpu_create_imag", "ses_gpu_relax",
-    "ses_gpu_step_driven",
+    "ses_gpu_step_driven", "ses_gpu_snapshot", "ses_gpu_restore", "ses_gpu_density_slice",
 ]
 
 
@@ -104,6 +104,9 @@ def _load() -> C.CDLL:
                                  C.POINTER(hp)], st),
         "ses_gpu_relax": ([hp, C.c_int, C.c_int, dp], st),
         "ses_gpu_step_driven": ([hp, C.c_int, C.c_int, dp, C.c_double, C.c_double, C.c_double], st),
+        "ses_gpu_snapshot": ([hp, C.c_int64, vp, C.c_size_t, C.POINTER(C.c_size_t)], st),
+        "ses_gpu_restore": ([hp, vp, C.c_size_t, C.POINTER(C.c_int64)], st),
+        "ses_gpu_density_slice": ([hp, C.c_int, C.c_int, C.POINTER(C.c_float)], st),
         "ses_gpu_set_potential": ([hp, dp], st),
         "ses_gpu_set_absorber": ([hp, dp], st),
         "ses_gpu_set_absorber_separable": ([hp, dp, dp, dp], st),

@@ -257,6 +257,26 @@ class SplitOperator3D:
         check(lib.ses_gpu_step_driven(self._h, int(nsteps), 1 if absorb else 0, ax.ctypes.data_as(_dp),
                                       float(amplitude), float(omega), float(t0)))
 
+    def snapshot(self, steps: int = 0) -> bytes:
+        """psi snapshot: 128-byte header + psi in the handle's precision (no conversion)."""
+        n = C.c_size_t()
+        check(lib.ses_gpu_snapshot(self._h, int(steps), None, 0, C.byref(n)))
+        buf = (C.c_char * n.value)()
+        check(lib.ses_gpu_snapshot(self._h, int(steps), buf, n.value, C.byref(n)))
+        return bytes(buf)
+
+    def restore(self, snap: bytes) -> int:
+        steps = C.c_int64()
+        check(lib.ses_gpu_restore(self._h, snap, len(snap), C.byref(steps)))
+        return steps.value
+
+    def density_slice(self, axis: int, index: int) -> np.ndarray:
+        dims = self.grid.dims
+        shape = [dims[a] for a in range(3) if a != axis]
+        out = np.empty(shape[0] * shape[1], dtype=np.float32)
+        check(lib.ses_gpu_density_slice(self._h, int(axis), int(index), out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out.reshape(shape[1], shape[0])
+
     def set_absorber(self, mask) -> None:
         if mask is None:
             check(lib.ses_gpu_set_absorber(self._h, None))

@@ -84,6 +84,22 @@ __global__ void renormalize_kernel(cx<T>* psi, long long N, const double* __rest
         psi[i] = scale_d(psi[i], s);
 }
 
+// |psi|^2 of the plane index `at` along `axis` (0/1/2) of an nx x ny x nz field,
+// the other two axes in their own order (first the lower axis), as FP32.
+template <typename T>
+__global__ void density_slice_kernel(const cx<T>* __restrict__ psi, int nx, int ny, int nz, int axis, int at,
+                                     float* out) {
+    const int na = axis == 0 ? ny : nx, nb = axis == 2 ? ny : nz;
+    const long long cnt = (long long)na * nb;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cnt;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(t % na), b = (int)(t / na);
+        const int i = axis == 0 ? at : a, j = axis == 0 ? a : (axis == 1 ? at : b), k = axis == 2 ? at : b;
+        const cx<double> p = widen(psi[i + (long long)nx * (j + (long long)ny * k)]);
+        out[t] = (float)(p.x * p.x + p.y * p.y);
+    }
+}
+
 // per-axis wavenumbers k_j = (2 pi / L) * (j if 2j < n else j - n)  (spectral.ixx:14-23)
 // and kinetic deltas cis(-k^2 dt/(2m)) - 1
 __global__ void build_axis_tables(double xmin, double xmax, int n, double dt, double mass,

@@ -499,13 +499,18 @@ ses_status pass_x(const ses_solver* h, const void* src, void* dst, const XProg& 
     a.m_mid = p.m_mid;
     a.m_store = p.m_store;
     a.out_scale = p.out_scale;
-    if (p.kick != 0.0) {
+    if (p.kick != 0.0) {  // driven step: the run-time-plan x pass carries the dipole kick
         a.tb.kick = p.kick;
         for (int q = 0; q < 3; ++q) {
             a.tb.kax[q] = p.kick_axis[q];
             a.tb.korg[q] = h->box[2 * q];
             a.tb.kh[q] = (h->box[2 * q + 1] - h->box[2 * q]) / phys_n(h, q);
         }
+        const PassPlan& pp = h->pp[0];
+        xkernel<T>(p.mode)<<<pp.grid, pp.g.nthreads, pp.smem, s>>>(a);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return fail(SES_EDEVICE, std::string("driven x pass launch: ") + cudaGetErrorString(e));
+        return SES_OK;
     }
     return launch<T>(h, 0, p.mode, a, s);
 }
@@ -2239,6 +2244,78 @@ ses_status ses_gpu_read_psi(ses_handle h, double* psi_out) {
         SES_CU(cudaGetLastError());
         SES_CU(cudaMemcpyAsync(psi_out + 2 * off, h->scratch, cnt * 16, cudaMemcpyDeviceToHost, h->stream));
     }
+    return wait_bounded(h, 0);
+}
+
+// Snapshot wire format: a 128-byte header, then psi in the handle's own precision
+// (interleaved float or double pairs, x fastest, as Engine::readback/upload_state).
+namespace {
+struct SnapHeader {
+    char magic[8];       // "SESPSI1"
+    int32_t prec;        // ses_precision
+    int32_t n[3];
+    double box[6];
+    double dt, mass;
+    int64_t steps;       // caller's step counter
+    char pad[128 - 8 - 4 - 12 - 48 - 16 - 8];
+};
+static_assert(sizeof(SnapHeader) == 128, "snapshot header is 128 bytes");
+}  // namespace
+
+ses_status ses_gpu_snapshot(ses_handle h, int64_t steps, void* out, size_t cap, size_t* bytes) {
+    SES_TRY(check_handle(h));
+    const size_t need = sizeof(SnapHeader) + (size_t)h->N * h->esize;
+    if (bytes) *bytes = need;
+    if (!out) return SES_OK;  // size query
+    if (cap < need) return fail(SES_EINVAL, "snapshot buffer too small: " + std::to_string(need) + " bytes needed");
+    SnapHeader hd{};
+    std::memcpy(hd.magic, "SESPSI1", 8);
+    hd.prec = h->prec;
+    for (int a = 0; a < 3; ++a) hd.n[a] = phys_n(h, a);
+    for (int a = 0; a < 6; ++a) hd.box[a] = h->box[a];
+    hd.dt = h->dt;
+    hd.mass = h->mass;
+    hd.steps = steps;
+    std::memcpy(out, &hd, sizeof(hd));
+    SES_CU(cudaMemcpyAsync(static_cast<char*>(out) + sizeof(hd), h->psi, (size_t)h->N * h->esize,
+                           cudaMemcpyDeviceToHost, h->stream));
+    return wait_bounded(h, 0);
+}
+
+ses_status ses_gpu_restore(ses_handle h, const void* snap, size_t bytes, int64_t* steps) {
+    SES_TRY(check_handle(h));
+    if (!snap || bytes < sizeof(SnapHeader)) return fail(SES_EINVAL, "not a snapshot");
+    SnapHeader hd;
+    std::memcpy(&hd, snap, sizeof(hd));
+    if (std::memcmp(hd.magic, "SESPSI1", 8) != 0) return fail(SES_EINVAL, "not a snapshot (bad magic)");
+    if (hd.prec != h->prec) return fail(SES_EINVAL, "snapshot precision differs from the handle's");
+    for (int a = 0; a < 3; ++a)
+        if (hd.n[a] != phys_n(h, a)) return fail(SES_EINVAL, "snapshot grid differs from the handle's");
+    if (bytes < sizeof(SnapHeader) + (size_t)h->N * h->esize) return fail(SES_EINVAL, "snapshot is truncated");
+    if (steps) *steps = hd.steps;
+    SES_CU(cudaMemcpyAsync(h->psi, static_cast<const char*>(snap) + sizeof(hd), (size_t)h->N * h->esize,
+                           cudaMemcpyHostToDevice, h->stream));
+    return wait_bounded(h, 0);
+}
+
+ses_status ses_gpu_density_slice(ses_handle h, int axis, int index, float* out) {
+    SES_TRY(check_handle(h));
+    if (!out) return fail(SES_EINVAL, "null output");
+    if (axis < 0 || axis > 2) return fail(SES_EINVAL, "axis must be 0, 1 or 2");
+    const int nx = phys_n(h, 0), ny = phys_n(h, 1), nz = phys_n(h, 2);
+    const int na[3] = {nx, ny, nz};
+    if (index < 0 || index >= na[axis]) return fail(SES_EINVAL, "slice index out of range");
+    const long long cnt = (long long)(axis == 0 ? ny : nx) * (axis == 2 ? ny : nz);
+    float* d = reinterpret_cast<float*>(h->scratch);  // N * esize bytes >= cnt floats
+    const unsigned gb = (unsigned)std::min<long long>((cnt + 255) / 256, 148 * 8);
+    if (h->prec == SES_C128)
+        density_slice_kernel<double><<<gb, 256, 0, h->stream>>>(reinterpret_cast<const cx<double>*>(h->psi), nx, ny,
+                                                                nz, axis, index, d);
+    else
+        density_slice_kernel<float><<<gb, 256, 0, h->stream>>>(reinterpret_cast<const cx<float>*>(h->psi), nx, ny,
+                                                               nz, axis, index, d);
+    SES_CU(cudaGetLastError());
+    SES_CU(cudaMemcpyAsync(out, d, (size_t)cnt * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     return wait_bounded(h, 0);
 }
 

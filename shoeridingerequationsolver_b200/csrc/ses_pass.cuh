@@ -94,13 +94,14 @@ template <typename T>
 __device__ __forceinline__ cx<T> apply_diag_tv(cx<T> v, int kind, cx<T> tab, int use_mask, double m);
 
 // Dipole kick of cell (i, j, k): psi * cis(-kick (ax x + ay y + az z)), the phase in FP64;
-// complex64 multiplies in FP32 on the delta form.
+// complex64 multiplies in FP32 on the delta form.  Out of line: the FP64 sincos
+// stays out of the passes' register allocation, which only test kick != 0.
 template <typename T>
-__device__ __forceinline__ cx<T> kick_mul(cx<T> v, const Tables& tb, int i, int j, int k) {
-    if (tb.kick == 0.0) return v;
-    const double u = tb.kax[0] * (tb.korg[0] + i * tb.kh[0]) + tb.kax[1] * (tb.korg[1] + j * tb.kh[1]) +
-                     tb.kax[2] * (tb.korg[2] + k * tb.kh[2]);
-    const double ang = -tb.kick * u;
+__device__ __noinline__ cx<T> kick_apply(cx<T> v, double kick, double ax, double ay, double az, double x0,
+                                         double y0, double z0, double hx, double hy, double hz, int i, int j,
+                                         int k) {
+    const double u = ax * (x0 + i * hx) + ay * (y0 + j * hy) + az * (z0 + k * hz);
+    const double ang = -kick * u;
     if constexpr (sizeof(T) == 4) {
         double s2, c2;
         sincos(0.5 * ang, &s2, &c2);
@@ -112,12 +113,28 @@ __device__ __forceinline__ cx<T> kick_mul(cx<T> v, const Tables& tb, int i, int 
     }
 }
 
-// psi * (potential phase) * (mask) * (dipole kick) at flat index f, coordinates (i, j, k).
+template <typename T>
+__device__ __forceinline__ cx<T> kick_mul(cx<T> v, const Tables& tb, int i, int j, int k) {
+    if (tb.kick == 0.0) return v;
+    return kick_apply<T>(v, tb.kick, tb.kax[0], tb.kax[1], tb.kax[2], tb.korg[0], tb.korg[1], tb.korg[2], tb.kh[0],
+                         tb.kh[1], tb.kh[2], i, j, k);
+}
+
+// psi * (potential phase) * (mask) at flat index f, coordinates (i, j, k).
 template <typename T>
 __device__ __forceinline__ cx<T> apply_diag(cx<T> v, int kind, int use_mask, long long f, int i, int j,
                                             int k, const Tables& tb) {
     const cx<T> tab = kind != DG_NONE ? reinterpret_cast<const cx<T>*>(tb.vtab)[f] : v;
-    return kick_mul(apply_diag_tv(v, kind, tab, use_mask, use_mask ? maskval<T>(tb, f, i, j, k) : 1.0), tb, i, j, k);
+    return apply_diag_tv(v, kind, tab, use_mask, use_mask ? maskval<T>(tb, f, i, j, k) : 1.0);
+}
+
+// The same and the dipole kick: only the run-time-plan x pass carries the kick,
+// which keeps its FP64 phase code out of the compiled passes' register budget
+// (driven steps always run their x passes on those kernels).
+template <typename T>
+__device__ __forceinline__ cx<T> apply_diag_kick(cx<T> v, int kind, int use_mask, long long f, int i, int j,
+                                                 int k, const Tables& tb) {
+    return kick_mul(apply_diag(v, kind, use_mask, f, i, j, k, tb), tb, i, j, k);
 }
 
 // Same as apply_diag with the potential-table entry and mask value supplied
@@ -284,7 +301,7 @@ __global__ void __launch_bounds__(512, 1) xpass_kernel(const PassArgs<T> a) {
                 if (a.d_load != DG_NONE || a.m_load) {
                     const int k = (int)fdiv((uint32_t)m, a.fny);
                     const int j = (int)(m - (long long)k * a.ny);
-                    v = apply_diag(v, a.d_load, a.m_load, f, e, j, k, a.tb);
+                    v = apply_diag_kick(v, a.d_load, a.m_load, f, e, j, k, a.tb);
                 }
             }
         }
@@ -311,7 +328,7 @@ __global__ void __launch_bounds__(512, 1) xpass_kernel(const PassArgs<T> a) {
                     const int k = (int)fdiv((uint32_t)m, a.fny);
                     const int j = (int)(m - (long long)k * a.ny);
                     sm[l * g.ls + e] =
-                        apply_diag(sm[l * g.ls + e], a.d_mid, a.m_mid, m * n + e, e, j, k, a.tb);
+                        apply_diag_kick(sm[l * g.ls + e], a.d_mid, a.m_mid, m * n + e, e, j, k, a.tb);
                 }
             }
             __syncthreads();
@@ -362,7 +379,7 @@ __global__ void __launch_bounds__(512, 1) xpass_kernel(const PassArgs<T> a) {
                 if (a.d_store != DG_NONE || a.m_store) {
                     const int k = (int)fdiv((uint32_t)m, a.fny);
                     const int j = (int)(m - (long long)k * a.ny);
-                    v = apply_diag(v, a.d_store, a.m_store, f, e, j, k, a.tb);
+                    v = apply_diag_kick(v, a.d_store, a.m_store, f, e, j, k, a.tb);
                 }
             }
             a.dst[f] = v;

@@ -239,7 +239,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
         if (vrow) {
             const cx<T> tab = kind != DG_NONE ? vrow[pos] : e;
             const double mv = !msk ? 1.0 : (mfull ? mfull[f] : mx[pos] * myz);
-            return kick_mul(apply_diag_tv(e, kind, tab, msk, mv), a.tb, pos, jy, kz);
+            return apply_diag_tv(e, kind, tab, msk, mv);
         }
         return apply_diag(e, kind, msk, f, pos, jy, kz, a.tb);
     };

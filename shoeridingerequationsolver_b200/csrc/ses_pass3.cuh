@@ -54,6 +54,7 @@ __device__ __forceinline__ void pipe_abort(const PipeArgs& pa, const uint64_t* b
 // memory; tile t is tile t mod bpi of instance t / bpi).
 template <typename T>
 struct OneField {
+    static constexpr bool kMany = false;
     const PassArgs<T>& a;
     const CUtensorMap* map;
     __device__ __forceinline__ const PassArgs<T>& args(uint32_t) const { return a; }
@@ -63,6 +64,7 @@ struct OneField {
 
 template <typename T>
 struct ManyFields {
+    static constexpr bool kMany = true;
     const PassArgs<T>* __restrict__ arr;
     const CUtensorMap* maps;
     BatchWork w;
@@ -86,8 +88,11 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
     cx<T>* tiles = reinterpret_cast<cx<T>*>(smraw3);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smraw3 + (size_t)NBUF * TILE_BYTES);
     using TW = TwStage<T, R0, R1, R2>;
-    cx<T>* twh = reinterpret_cast<cx<T>*>(smraw3 + pipe_tw_offset((size_t)NBUF * TILE_BYTES, NBUF));
-    const cx<T>* twl = TW::lo_of(twh);
+    // many fields: one shared-memory copy of the class's twiddles; one field: its tables via L1
+    constexpr bool kSmemTw = F::kMany;
+    cx<T>* tws = reinterpret_cast<cx<T>*>(smraw3 + pipe_tw_offset((size_t)NBUF * TILE_BYTES, NBUF));
+    const cx<T>* twh = kSmemTw ? tws : f.args(blockIdx.x).stw;
+    const cx<T>* twl = kSmemTw ? TW::lo_of(tws) : f.args(blockIdx.x).stwl;
     const int l = threadIdx.x % L, q = threadIdx.x / L;
     const int nmine = blockIdx.x < (unsigned)pa.ntiles ? (pa.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
@@ -95,7 +100,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
         for (int b = 0; b < NBUF; ++b) mbar_init(smem_u32(&bars[b]), 1);
         fence_mbar_init();
     }
-    if (nmine > 0) TW::load(twh, f.args(blockIdx.x).stw, f.args(blockIdx.x).stwl);
+    if (kSmemTw && nmine > 0) TW::load(tws, f.args(blockIdx.x).stw, f.args(blockIdx.x).stwl);
     __syncthreads();
     auto issue = [&](int i) {  // thread 0: load this CTA's i-th tile into buffer i % NBUF
         const int buf = i % NBUF;
@@ -235,8 +240,10 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
     extern __shared__ __align__(1024) unsigned char smraw3[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smraw3 + (size_t)NBUF * BUF_BYTES);
     using TW = TwStage<T, R0, R1, R2>;
-    cx<T>* twh = reinterpret_cast<cx<T>*>(smraw3 + pipe_tw_offset((size_t)NBUF * BUF_BYTES, NBUF));
-    const cx<T>* twl = TW::lo_of(twh);
+    constexpr bool kSmemTw = F::kMany;
+    cx<T>* tws = reinterpret_cast<cx<T>*>(smraw3 + pipe_tw_offset((size_t)NBUF * BUF_BYTES, NBUF));
+    const cx<T>* twh = kSmemTw ? tws : f.args(blockIdx.x).stw;
+    const cx<T>* twl = kSmemTw ? TW::lo_of(tws) : f.args(blockIdx.x).stwl;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int lw = lane / TL, q = lane % TL;
     const int nmine = blockIdx.x < (unsigned)pa.ntiles ? (pa.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -245,7 +252,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
         for (int b = 0; b < NBUF; ++b) mbar_init(smem_u32(&bars[b]), 1);
         fence_mbar_init();
     }
-    if (nmine > 0) TW::load(twh, f.args(blockIdx.x).stw, f.args(blockIdx.x).stwl);
+    if (kSmemTw && nmine > 0) TW::load(tws, f.args(blockIdx.x).stw, f.args(blockIdx.x).stwl);
     __syncthreads();
     auto issue = [&](int i) {
         const int buf = i % NBUF;
@@ -303,8 +310,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                 cx<T> e = line[pos];
                 if constexpr (MODE == XM_START || MODE == XM_1D) {
                     if (a.d_load != DG_NONE || a.m_load)
-                        e = kick_mul(apply_diag_tv(e, a.d_load, tline[pos], a.m_load, a.m_load ? mval(pos) : 1.0),
-                                     a.tb, pos, jy, kz);
+                        e = apply_diag_tv(e, a.d_load, tline[pos], a.m_load, a.m_load ? mval(pos) : 1.0);
                 }
                 v[b * RF + r] = kConjIn ? cconj(e) : e;
             }
@@ -322,9 +328,8 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                         if constexpr (MODE == XM_END) {
                             e = cconj(e);
                             if (a.d_store != DG_NONE || a.m_store)
-                                e = kick_mul(apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
-                                                           a.m_store ? mval(pos) : 1.0),
-                                             a.tb, pos, jy, kz);
+                                e = apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
+                                                  a.m_store ? mval(pos) : 1.0);
                         }
                         dst[pos] = e;
                     }
@@ -340,8 +345,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                     if constexpr (MODE == XM_MID) {
                         e = cconj(e);
                         if (a.d_mid != DG_NONE || a.m_mid)
-                            e = kick_mul(apply_diag_tv(e, a.d_mid, tline[pos], a.m_mid, a.m_mid ? mval(pos) : 1.0),
-                                         a.tb, pos, jy, kz);
+                            e = apply_diag_tv(e, a.d_mid, tline[pos], a.m_mid, a.m_mid ? mval(pos) : 1.0);
                     } else {
                         e = kinetic_conj(e, dmul1(dyz, a.tb.kd[0][pos]), a.tb.kscale);
                     }
@@ -358,9 +362,8 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                         if constexpr (MODE == XM_1D) {
                             e = cconj(e);
                             if (a.d_store != DG_NONE || a.m_store)
-                                e = kick_mul(apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
-                                                           a.m_store ? mval(pos) : 1.0),
-                                             a.tb, pos, jy, kz);
+                                e = apply_diag_tv(e, a.d_store, tline[pos], a.m_store,
+                                                  a.m_store ? mval(pos) : 1.0);
                         }
                         dst[pos] = e;
                     }
