@@ -353,13 +353,30 @@ def cpu_baseline_c4(specs, budget_s=15.0):
 # ---------------------------------------------------------------------------
 # C5: serving
 # ---------------------------------------------------------------------------
-def serve_run(ses, nreq, capacity_ptsteps, seed=None):
+def serve_capacity(ses, ncal=16):
+    """Closed-loop capacity of the server on this mix: a separate seeded draw of
+    `ncal` requests submitted at once; grid-pt*steps of all rounds / wall time."""
+    from shoeridingerequationsolver_b200 import scenes
+    built = [scenes.build_c5_request(s) for s in scenes.config_c5_specs(ncal, seed=scenes.SEED_BASE + 40)]
+    with ses.Server(budget_bytes=150 * 10**9, max_round_steps=100) as srv:
+        t0 = time.perf_counter()
+        for req in built:
+            srv.submit(**req)
+        srv.wait_idle(900000)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    return st["gridpt_steps"] / wall
+
+
+def serve_run(ses, nreq, capacity_ptsteps=None, seed=None):
     """Poisson arrivals of mixed 1D/2D/3D requests into the request server; lambda
-    set so the offered load is ~0.9 of `capacity_ptsteps` (grid-pt*steps/s)."""
+    set so the offered load is ~0.9 of the server's closed-loop capacity on the mix."""
     import numpy as np
     from shoeridingerequationsolver_b200 import scenes
     specs = scenes.config_c5_specs(nreq) if seed is None else scenes.config_c5_specs(nreq, seed=seed)
     mean_work = sum(s["points"] * s["steps"] for s in specs) / len(specs)
+    if capacity_ptsteps is None:
+        capacity_ptsteps = serve_capacity(ses)
     lam = 0.9 * capacity_ptsteps / mean_work
     rng = np.random.default_rng(scenes.SEED_BASE + 50)
     gaps = rng.exponential(1.0 / lam, len(specs))
@@ -392,7 +409,8 @@ def serve_run(ses, nreq, capacity_ptsteps, seed=None):
             "latency_p99_ms": round(float(np.percentile(lats, 99)), 2) if lats else None,
             "throughput": st["gridpt_steps"] / wall, "unit": UNIT, "wall_s": round(wall, 2),
             "rounds": st["rounds"], "records": nrec, "budget_bytes": 150 * 10**9,
-            "offered_load": "0.9 x the measured batched capacity"}
+            "capacity": capacity_ptsteps,
+            "offered_load": "0.9 x the server's closed-loop capacity on a separate draw of the mix"}
 
 
 # ---------------------------------------------------------------------------
@@ -624,7 +642,7 @@ def run_ours(args):
         if acc_steps > 0:
             line["accuracy"] = c4_accuracy(ses, specs, acc_steps)
         if not args.no_serve:
-            line["serve"] = serve_run(ses, args.serve_requests, value / world)
+            line["serve"] = serve_run(ses, args.serve_requests)
         if not args.no_single:
             w = scenes.config_c2(256)
             line["single_c2"] = single_line(ses, w, 200, 3, stream, peak, peak_kind, traffic_table, clocks_gpu)

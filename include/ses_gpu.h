@@ -253,6 +253,9 @@ SES_API ses_status ses_batch_step(ses_batch b, int nsteps, int absorb);
 /* ses_gpu_observe of every member, in the order they were added (count must be
  * the member count), with one wait for the whole batch. */
 SES_API ses_status ses_batch_observe(ses_batch b, double xlo, double xhi, ses_observables* out, int count);
+/* The same for the listed members only, each with its own x-interval. */
+SES_API ses_status ses_batch_observe_some(ses_batch b, const ses_handle* hs, int count, const double* xlo,
+                                          const double* xhi, ses_observables* out);
 SES_API ses_status ses_batch_sync(ses_batch b, int timeout_ms);
 SES_API ses_status ses_batch_set_stream(ses_batch b, void* cuda_stream);
 SES_API ses_status ses_batch_members(ses_batch b, int* members, int* classes);

@@ -1454,8 +1454,23 @@ enum BatchProg {
     BP_1DLAST,  // 1D [V (M), fwd, K/N, inv, Vh (M)]
     BP_NX,
     BP_MID0 = BP_NX,  // strided passes of the step, in order
-    BP_COUNT = BP_NX + 3
+    BP_LSTART = BP_NX + 3,  // long line: [Vh, fwd y, * W]
+    BP_LX,                  // long line: [fwd x, K/N, inv x]
+    BP_LMID,                // long line: [* conj W, inv y, V (M), fwd y, * W]
+    BP_LEND,                // long line: [* conj W, inv y, Vh (M)]
+    BP_COUNT
 };
+
+// Axis, mode and potential/mask program of a long-line program.
+void long_prog(int prog, bool mask, int* axis, int* mode, XProg* p) {
+    *p = XProg();
+    switch (prog) {
+        case BP_LSTART: *axis = 1; *mode = SM_TW_START; p->d_load = DG_HALF; break;
+        case BP_LX: *axis = 0; *mode = XM_1D; break;
+        case BP_LMID: *axis = 1; *mode = SM_TW_MID; p->d_mid = DG_FULL; p->m_mid = mask; break;
+        default: *axis = 1; *mode = SM_TW_END; p->d_store = DG_HALF; p->m_store = mask; break;
+    }
+}
 
 XProg batch_xprog(int prog, bool mask) {
     XProg p;
@@ -1553,7 +1568,11 @@ ses_status batch_wait(ses_batch_s* b, int timeout_ms) {
 template <typename T>
 bool class_has_batch_kernels(const BatchClass& c) {
     const ses_solver* h = c.mem[0];
-    if (h->long1d) return false;  // long lines step member by member
+    if (h->long1d) {  // four-step programs: contiguous XM_1D and the strided SM_TW_* passes
+        const auto* ex = reinterpret_cast<const PlanEntry<T>*>(h->pp[0].cp);
+        const auto* ey = reinterpret_cast<const PlanEntry<T>*>(h->pp[1].cp);
+        return ex && ey && ex->xb[XM_1D] && ey->sb[SM_TW_START] && ey->sb[SM_TW_MID] && ey->sb[SM_TW_END];
+    }
     for (int a = 0; a < 3; ++a) {
         if (h->n[a] < 2 && a > 0) continue;
         if (h->n[a] < 2) return false;  // a 1-point x axis has no compiled plan
@@ -1698,6 +1717,13 @@ ses_status class_upload(const ses_batch_s* b, BatchClass& c) {
                     a.d_load = p.d_load; a.d_mid = p.d_mid; a.d_store = p.d_store;
                     a.m_load = p.m_load; a.m_mid = p.m_mid; a.m_store = p.m_store;
                     a.out_scale = p.out_scale;
+                } else if (prog >= BP_LSTART) {
+                    int ax, md;
+                    XProg p;
+                    long_prog(prog, m, &ax, &md, &p);
+                    a = make_args<T>(h, ax, h->psi, h->psi);
+                    a.d_load = p.d_load; a.d_mid = p.d_mid; a.d_store = p.d_store;
+                    a.m_load = p.m_load; a.m_mid = p.m_mid; a.m_store = p.m_store;
                 } else if (prog - BP_MID0 < c.nmid) {
                     a = make_args<T>(h, c.mid_axis[prog - BP_MID0], h->psi, h->psi);
                 } else {
@@ -1730,8 +1756,12 @@ template <typename T>
 ses_status class_launch(const ses_batch_s* b, const BatchClass& c, int prog, bool mask, cudaStream_t s,
                         const PassArgs<T>* args_ovr = nullptr, const CUtensorMap* maps_ovr = nullptr) {
     const ses_solver* h0 = c.mem[0];
-    const int axis = prog < BP_NX ? 0 : c.mid_axis[prog - BP_MID0];
-    const int mode = prog < BP_NX ? batch_xprog(prog, mask).mode : c.mid_mode[prog - BP_MID0];
+    int axis = prog < BP_NX ? 0 : (prog >= BP_LSTART ? 1 : c.mid_axis[prog - BP_MID0]);
+    int mode = prog < BP_NX ? batch_xprog(prog, mask).mode : (prog >= BP_LSTART ? 0 : c.mid_mode[prog - BP_MID0]);
+    if (prog >= BP_LSTART) {
+        XProg unused;
+        long_prog(prog, mask, &axis, &mode, &unused);
+    }
     const PassPlan& pp = h0->pp[axis];
     const auto* e = reinterpret_cast<const PlanEntry<T>*>(pp.cp);
     const size_t nm = c.mem.size();
@@ -1739,8 +1769,8 @@ ses_status class_launch(const ses_batch_s* b, const BatchClass& c, int prog, boo
         args_ovr ? args_ovr : reinterpret_cast<const PassArgs<T>*>(c.dargs) + ((size_t)prog * 2 + (mask ? 1 : 0)) * nm;
     const CUtensorMap* maps = maps_ovr ? maps_ovr : c.dmaps;
     const int q = prog - BP_MID0;
-    if (axis == 0 ? c.xvar >= 0 && (mode == XM_START || mode == XM_MID || mode == XM_END)
-                  : c.svar[q] >= 0) {
+    if (prog < BP_LSTART && (axis == 0 ? c.xvar >= 0 && (mode == XM_START || mode == XM_MID || mode == XM_END)
+                                       : c.svar[q] >= 0)) {
         const int n = h0->n[axis];
         PipeArgs pa{};
         pa.err = b->derr;
@@ -1796,6 +1826,10 @@ ses_status class_launch(const ses_batch_s* b, const BatchClass& c, int prog, boo
 
 template <typename T>
 ses_status class_unit(const ses_batch_s* b, const BatchClass& c, bool mask, cudaStream_t s) {
+    if (c.mem[0]->long1d) {
+        SES_TRY(class_launch<T>(b, c, BP_LMID, mask, s));
+        return class_launch<T>(b, c, BP_LX, mask, s);
+    }
     if (c.mem[0]->last_axis == 0) return class_launch<T>(b, c, BP_1DMID, mask, s);
     SES_TRY(class_launch<T>(b, c, BP_XMID, mask, s));
     for (int q = 0; q < c.nmid; ++q) SES_TRY(class_launch<T>(b, c, BP_MID0 + q, mask, s));
@@ -1830,8 +1864,13 @@ ses_status class_body(const ses_batch_s* b, BatchClass& c, bool mask) {
 template <typename T>
 ses_status class_steps(const ses_batch_s* b, BatchClass& c, int S, bool mask, cudaStream_t s) {
     const bool one_d = c.mem[0]->last_axis == 0;
+    const bool long1d = c.mem[0]->long1d;
     int interior;
-    if (one_d) {
+    if (long1d) {
+        SES_TRY(class_launch<T>(b, c, BP_LSTART, mask, s));
+        SES_TRY(class_launch<T>(b, c, BP_LX, mask, s));
+        interior = S - 1;
+    } else if (one_d) {
         if (S == 1) return class_launch<T>(b, c, BP_1DONE, mask, s);
         SES_TRY(class_launch<T>(b, c, BP_1DFIRST, mask, s));
         interior = S - 2;
@@ -1846,7 +1885,7 @@ ses_status class_steps(const ses_batch_s* b, BatchClass& c, int S, bool mask, cu
         interior -= kBodyUnroll;
     }
     for (; interior > 0; --interior) SES_TRY(class_unit<T>(b, c, mask, s));
-    return class_launch<T>(b, c, one_d ? BP_1DLAST : BP_XEND, mask, s);
+    return class_launch<T>(b, c, long1d ? BP_LEND : (one_d ? BP_1DLAST : BP_XEND), mask, s);
 }
 
 // Regroup members into classes and refresh the argument tables of changed ones.
@@ -1881,7 +1920,7 @@ template <typename T>
 ses_status class_autotune(ses_batch_s* b, BatchClass& c, std::map<std::string, int>& chosen) {
     const size_t nm = c.mem.size();
     const ses_solver* h0 = c.mem[0];
-    if (!c.batched || h0->last_axis == 0) return SES_OK;
+    if (!c.batched || h0->last_axis == 0 || h0->long1d) return SES_OK;
     std::vector<PassArgs<T>> host(nm * (1 + (size_t)c.nmid));
     for (size_t i = 0; i < nm; ++i) {
         const ses_solver* h = c.mem[i];
@@ -2542,6 +2581,21 @@ ses_status ses_batch_info(ses_batch b, char* buf, size_t len) {
     return SES_OK;
 }
 
+ses_status ses_batch_observe_some(ses_batch b, const ses_handle* hs, int count, const double* xlo,
+                                  const double* xhi, ses_observables* out) {
+    SES_TRY(check_batch(b));
+    if (count < 0 || (count > 0 && (!hs || !xlo || !xhi || !out))) return fail(SES_EINVAL, "null argument");
+    for (int i = 0; i < count; ++i)
+        if (!hs[i] || hs[i]->batch != b) return fail(SES_EINVAL, "handle is not a member of this batch");
+    for (int i = 0; i < count; ++i) {
+        ses_solver* h = hs[i];
+        SES_TRY(h->prec == SES_C128 ? enqueue_observe<double>(h, xlo[i], xhi[i]) : enqueue_observe<float>(h, xlo[i], xhi[i]));
+    }
+    SES_TRY(batch_wait(b, 0));
+    for (int i = 0; i < count; ++i) finish_observe(hs[i], &out[i]);
+    return SES_OK;
+}
+
 ses_status ses_batch_sync(ses_batch b, int timeout_ms) {
     SES_TRY(check_batch(b));
     return batch_wait(b, timeout_ms);
@@ -2573,7 +2627,7 @@ ses_status ses_batch_profile(ses_batch b, int nsteps, int absorb, double* ms, in
         BatchClass* c = b->classes[ci];
         double* o = ms + 5 * ci;
         for (int q = 0; q < 5; ++q) o[q] = 0.0;
-        if (!c->batched) continue;
+        if (!c->batched || c->mem[0]->long1d) continue;
         const bool one_d = c->mem[0]->last_axis == 0;
         std::vector<int> progs;
         progs.push_back(one_d ? (int)BP_1DMID : (int)BP_XMID);

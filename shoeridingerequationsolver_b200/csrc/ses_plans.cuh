@@ -94,6 +94,9 @@ PlanEntry<T> make_plan_entry() {
     p.sb[SM_FWD] = sbatch_kernel<T, SM_FWD, N, E, R0, R1, R2, LS>;
     p.sb[SM_INV] = sbatch_kernel<T, SM_INV, N, E, R0, R1, R2, LS>;
     p.sb[SM_FUSED] = sbatch_kernel<T, SM_FUSED, N, E, R0, R1, R2, LS>;
+    p.sb[SM_TW_START] = sbatch_kernel<T, SM_TW_START, N, E, R0, R1, R2, LS>;
+    p.sb[SM_TW_MID] = sbatch_kernel<T, SM_TW_MID, N, E, R0, R1, R2, LS>;
+    p.sb[SM_TW_END] = sbatch_kernel<T, SM_TW_END, N, E, R0, R1, R2, LS>;
     for (int m = 0; m < 7; ++m)
         if (p.xb[m]) {
             allow_smem(p.xb[m], (int)p.xbsm);

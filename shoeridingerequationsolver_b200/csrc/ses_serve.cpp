@@ -261,20 +261,35 @@ void worker_main(ses_server_s* s) {
             s->gridpt_steps += pts;
             s->busy_ms += round_ms;
         }
+        // observations of this round: every member at an observation point or done, one wait
+        std::vector<ses_handle> oh;
+        std::vector<double> olo, ohi;
+        std::vector<size_t> oi;
+        for (size_t i = 0; i < s->active.size(); ++i) {
+            Request& r = *s->active[i];
+            r.done += R;
+            if (r.done >= r.nsteps || (r.every > 0 && r.done % r.every == 0)) {
+                oh.push_back(r.h);
+                olo.push_back(r.xlo);
+                ohi.push_back(r.xhi);
+                oi.push_back(i);
+            }
+        }
+        std::vector<ses_observables> obs(oh.size());
+        if (!oh.empty()) st = ses_batch_observe_some(s->batch, oh.data(), (int)oh.size(), olo.data(), ohi.data(), obs.data());
+        if (st != SES_OK) {
+            const std::string err = ses_last_error();
+            for (const auto& r : s->active) retire(s, r, SES_REQ_FAILED, err);
+            s->active.clear();
+            continue;
+        }
+        for (size_t q = 0; q < oi.size(); ++q) {
+            Request& r = *s->active[oi[q]];
+            push_record(s, r, obs[q], r.done >= r.nsteps);
+        }
         for (size_t i = 0; i < s->active.size();) {
             std::shared_ptr<Request> r = s->active[i];
-            r->done += R;
             const bool fin = r->done >= r->nsteps;
-            if (fin || (r->every > 0 && r->done % r->every == 0)) {
-                ses_observables o{};
-                st = ses_gpu_observe(r->h, r->xlo, r->xhi, &o);
-                if (st != SES_OK) {
-                    retire(s, r, SES_REQ_FAILED, ses_last_error());
-                    s->active.erase(s->active.begin() + (long)i);
-                    continue;
-                }
-                push_record(s, *r, o, fin);
-            }
             if (fin) {
                 std::vector<double> out((size_t)grid_points(r->grid) * 2);
                 st = ses_gpu_read_psi(r->h, out.data());

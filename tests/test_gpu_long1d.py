@@ -78,3 +78,24 @@ def test_long_line_observables_and_tables(ses, oracle):
     with pytest.raises(ValueError):
         op.fft3()
     op.close()
+
+
+@pytest.mark.gpu
+def test_long_lines_in_a_batch_match_alone(ses, oracle):
+    """Long lines form their own batch class (one launch per four-step pass for all
+    of them); each member ends exactly where it ends stepped alone."""
+    members, alone = [], []
+    for pot in ("morse", "double_well", "morse"):
+        a, V, psi, m = line(ses, oracle, "c64", pot, mask=True)
+        b, _, _, _ = line(ses, oracle, "c64", pot, mask=True)
+        members.append(a)
+        alone.append(b)
+    with ses.Batch(members) as bt:
+        assert bt.counts() == (3, 1)
+        bt.step(23, absorb=True)
+        bt.sync()
+        for a, b in zip(members, alone):
+            b.advance(23, absorb=True)
+            assert np.array_equal(a.readback(), b.readback())
+    for op in members + alone:
+        op.close()
