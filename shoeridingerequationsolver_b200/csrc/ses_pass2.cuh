@@ -143,12 +143,24 @@ __device__ __forceinline__ void rfft_plan(cx<T> (&v)[E], int q, const cx<T>* twh
     else rfft<T, N, E, S::v0, S::v1, S::v2, S::fwd_tables>(v, q, twh, twl, x);
 }
 
-template <typename T, int PITCH>
+// Padded line in shared memory: element pos at pos + PM * (pos >> SH).
+template <typename T, int SH, int PM>
 struct XchWarp {
     cx<T>* p;
-    __device__ __forceinline__ void put(int pos, cx<T> v) { p[pos + (pos >> 4)] = v; }
-    __device__ __forceinline__ cx<T> get(int pos) const { return p[pos + (pos >> 4)]; }
+    __device__ __forceinline__ void put(int pos, cx<T> v) { p[pos + PM * (pos >> SH)] = v; }
+    __device__ __forceinline__ cx<T> get(int pos) const { return p[pos + PM * (pos >> SH)]; }
     __device__ __forceinline__ void sync() { __syncwarp(); }
+};
+
+// Padding of the contiguous pass's lines: the layouts with the fewest shared-memory
+// wavefronts over every exchange of the plan (forward and reversed orders, both
+// half-warps of 64-bit accesses), found by modelling the access patterns.
+template <int N>
+struct XPad {
+    static constexpr int SH = N == 160 || N == 96 || N == 64 ? 3 : (N == 48 || N == 32 ? 2 : 4);
+    static constexpr int PM = N == 48 ? 3 : 1;
+    static constexpr int LPAD = N == 160 ? 4 : (N == 96 ? 12 : (N == 32 ? 4 : 0));
+    static constexpr int PITCH = N + PM * (N >> SH) + LPAD;
 };
 
 template <typename T, int L>
@@ -174,7 +186,7 @@ template <typename T, int N, int E>
 struct XShape {
     static constexpr int TL = N / E;
     static constexpr int LPW = 32 / TL;          // lines per warp
-    static constexpr int PITCH = N + N / 16;     // one pad element every 16
+    static constexpr int PITCH = XPad<N>::PITCH;
     static constexpr int per_warp = LPW * PITCH * (int)sizeof(cx<T>);
     static constexpr int NW = (48 * 1024) / per_warp >= 4 ? 4 : ((48 * 1024) / per_warp < 1 ? 1 : (48 * 1024) / per_warp);
 };
@@ -207,7 +219,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
     const long long mc = valid ? m : 0;
     const int kz = (int)fdiv((uint32_t)mc, a.fny);
     const int jy = (int)(mc - (long long)kz * a.ny);
-    XchWarp<T, PITCH> x{xb + (warp * LPW + lw) * PITCH};
+    XchWarp<T, XPad<N>::SH, XPad<N>::PM> x{xb + (warp * LPW + lw) * PITCH};
     const cx<T>* src = a.src + mc * N;
     cx<T>* dst = a.dst + mc * N;
     cx<T> v[E];

@@ -207,6 +207,15 @@ COMPILED_PLANS = [(16, 16, (16,)), (32, 8, (8, 4)), (48, 12, (4, 4, 3)), (64, 8,
                   (512, 16, (8, 8, 8)), (1024, 32, (16, 8, 8))]
 
 
+def xpad(N):
+    """Contiguous-pass line padding (ses_pass2.cuh XPad): element pos at pos + PM (pos >> SH),
+    line pitch N + PM (N >> SH) + LPAD."""
+    sh = 3 if N in (160, 96, 64) else (2 if N in (48, 32) else 4)
+    pm = 3 if N == 48 else 1
+    lpad = {160: 4, 96: 12, 32: 4}.get(N, 0)
+    return sh, pm, lpad
+
+
 def stage_table(N, rads):
     """Host table (ses_gpu.cu stage_twiddles): forward order then reversed order."""
     out = []
@@ -246,7 +255,8 @@ def model_fft(x, N, E, rads, tab, toff):
                     for r in range(R):
                         pos = (j - k) * R + k + r * Ns
                         assert 0 <= pos < N and np.isnan(buf[pos])  # each slot written once
-                        smem_max = max(smem_max, pos + pos // 16)
+                        sh, pm, _ = xpad(N)
+                        smem_max = max(smem_max, pos + pm * (pos >> sh))
                         buf[pos] = v[q][b * R + r]
             v = [[buf[q + TL * b + r * (N // Rn)] for b in range(E // Rn) for r in range(Rn)]
                  for q in range(TL)]
@@ -258,7 +268,8 @@ def model_fft(x, N, E, rads, tab, toff):
         for b in range(E // RL):
             for r in range(RL):
                 out[q + TL * b + r * (N // RL)] = v[q][b * RL + r]
-    assert smem_max < N + N // 16 or len(rads) == 1
+    sh, pm, lpad = xpad(N)
+    assert smem_max < N + pm * (N >> sh) + lpad or len(rads) == 1
     return out
 
 
