@@ -550,12 +550,10 @@ def run_ours(args):
     K, W = args.steps, max(args.warmup, 3)
     clocks_gpu = local if world > 1 else 0
 
-    def max_over_ranks(ms):
-        if not dist:
-            return ms
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from shoeridingerequationsolver_b200 import replicas
+
+    def max_over_ranks(ms):  # every rank runs its own replica of the workload (weak scaling)
+        return replicas.max_over_ranks(ms, dist, device="cuda")
 
     if args.config != "c4":  # single-instance workloads
         w = single_workload(args)
