@@ -476,6 +476,24 @@ def single_line(ses, w, K, W, stream, peak, peak_kind, traffic_table, clocks_gpu
     return out
 
 
+def other_configs(ses, stream, peak, peak_kind, traffic_table, clocks_gpu):
+    """The remaining named single-instance configurations at 1 GPU: C1 (64^3 harmonic,
+    plain FP64) and C3 (512^3 tunnelling, complex64, 1 GiB field)."""
+    from shoeridingerequationsolver_b200 import scenes
+    out = {}
+    for w, prec, K in ((scenes.config_c1(), "c128", 400), (scenes.config_c3(512), "c64", 50)):
+        r = single_precision(ses, w, prec, K, 3, stream, clocks_gpu)
+        npts = w.grid.size()
+        v = npts * K / (r["ms"] * 1e-3)
+        mb = MODEL_BYTES[(prec, 3)]
+        out[w.name] = {"precision": prec, "value": v, "ms_per_step": r["ms"] / K, "steps_timed": K,
+                       "step_model_frac": round(mb * v / 1e9 / peak, 4),
+                       "roofline": single_roofline(r["profile"], npts, prec, peak, peak_kind, traffic_table, w.name),
+                       "note": "64^3 complex128 fits in L2 (4 MiB): the model fraction can exceed 1" if npts < 2**20
+                       else "field and table far larger than L2"}
+    return out
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -644,6 +662,7 @@ def run_ours(args):
         if not args.no_single:
             w = scenes.config_c2(256)
             line["single_c2"] = single_line(ses, w, 200, 3, stream, peak, peak_kind, traffic_table, clocks_gpu)
+            line["configs"] = other_configs(ses, stream, peak, peak_kind, traffic_table, clocks_gpu)
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline_c4(specs)
     if dist:
