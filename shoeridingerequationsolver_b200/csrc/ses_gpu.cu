@@ -1793,7 +1793,7 @@ ses_status class_launch(const ses_batch_s* b, const BatchClass& c, int prog, boo
         if (axis == 0) {
             const auto& v = e->xv[c.xvar];
             const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * v.bbps[mode]));
-            v.kb[mode]<<<grid, 32 * v.warps, v.smem[mode], s>>>(args, w, pa);
+            v.kb[mode]<<<grid, 32 * v.warps, v.smemb[mode], s>>>(args, w, pa);
         } else {
             const auto& v = e->sv[c.svar[q]];
             const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * v.bbps[mode]));

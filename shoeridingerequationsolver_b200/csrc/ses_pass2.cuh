@@ -225,32 +225,43 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
     cx<T> v[E];
     constexpr bool kTabLate = MODE == XM_MID || MODE == XM_END;  // table used after the first FFT
     cx<T>* vrow = vt ? vt + (size_t)(warp * LPW + lw) * N : nullptr;
+    const double* mfull = a.tb.maskfull;
+    const double* mx = a.tb.mask1[0];
+    // this warp's copy of the x profile of a separable absorber (N doubles after the
+    // table rows of all warps), staged with the rows by the passes that use it
+    double* ms = vt ? reinterpret_cast<double*>(vt + (size_t)NW * LPW * N) + (size_t)warp * N : nullptr;
     if constexpr (kTabLate) {
         const bool want = MODE == XM_MID ? a.d_mid != DG_NONE : a.d_store != DG_NONE;
-        if (vt && want) {  // this warp's rows, 16-byte chunks spread over the lanes
+        const bool wantm = (MODE == XM_MID ? a.m_mid : a.m_store) && !mfull && mx;
+        if (vt && (want || wantm)) {  // this warp's rows, 16-byte chunks spread over the lanes
             __syncwarp();  // the previous tile's reads of these rows are done
-            constexpr int CH = N * (int)sizeof(cx<T>) / 16;
-            const long long m0 = (blk * NW + warp) * LPW;
-            const cx<T>* tab = reinterpret_cast<const cx<T>*>(a.tb.vtab);
-            for (int c = lane; c < LPW * CH; c += 32) {
-                const int ln = c / CH, ch = c - ln * CH;
-                if (m0 + ln < a.nlines)
-                    cp_async16(reinterpret_cast<char*>(vt + (size_t)(warp * LPW + ln) * N) + 16 * ch,
-                               reinterpret_cast<const char*>(tab + (m0 + ln) * N) + 16 * ch);
+            if (want) {
+                constexpr int CH = N * (int)sizeof(cx<T>) / 16;
+                const long long m0 = (blk * NW + warp) * LPW;
+                const cx<T>* tab = reinterpret_cast<const cx<T>*>(a.tb.vtab);
+                for (int c = lane; c < LPW * CH; c += 32) {
+                    const int ln = c / CH, ch = c - ln * CH;
+                    if (m0 + ln < a.nlines)
+                        cp_async16(reinterpret_cast<char*>(vt + (size_t)(warp * LPW + ln) * N) + 16 * ch,
+                                   reinterpret_cast<const char*>(tab + (m0 + ln) * N) + 16 * ch);
+                }
+            }
+            if (wantm) {
+                constexpr int MCH = N * (int)sizeof(double) / 16;
+                for (int c = lane; c < MCH; c += 32)
+                    cp_async16(reinterpret_cast<char*>(ms) + 16 * c, reinterpret_cast<const char*>(mx) + 16 * c);
             }
             cp_async_commit();
         }
     }
     // potential / mask at element pos of this line; the table entry from vrow when
     // prefetched, the separable mask as mx[pos] times the line's my[j] mz[k]
-    const double* mfull = a.tb.maskfull;
-    const double* mx = a.tb.mask1[0];
     const double myz = (!mfull && mx) ? a.tb.mask1[1][jy] * a.tb.mask1[2][kz] : 1.0;
     auto diag = [&](cx<T> e, int kind, int msk, int pos) {
         const long long f = mc * N + pos;
         if (vrow) {
             const cx<T> tab = kind != DG_NONE ? vrow[pos] : e;
-            const double mv = !msk ? 1.0 : (mfull ? mfull[f] : mx[pos] * myz);
+            const double mv = !msk ? 1.0 : (mfull ? mfull[f] : ms[pos] * myz);  // ms staged when msk
             return apply_diag_tv(e, kind, tab, msk, mv);
         }
         return apply_diag(e, kind, msk, f, pos, jy, kz, a.tb);
@@ -552,11 +563,13 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4)
     }
 }
 
-// Dynamic shared memory of xbatch_kernel: stage twiddles, then NW * LPW table rows.
+// Dynamic shared memory of xbatch_kernel: stage twiddles, then NW * LPW table
+// rows, then one x profile of the absorber (N doubles) per warp.
 template <typename T, int N, int E, int R0, int R1, int R2>
 constexpr size_t xbatch_smem() {
     return TwStage<T, R0, R1, R2>::bytes +
-           (size_t)XShape<T, N, E>::NW * XShape<T, N, E>::LPW * N * sizeof(cx<T>);
+           (size_t)XShape<T, N, E>::NW * XShape<T, N, E>::LPW * N * sizeof(cx<T>) +
+           (size_t)XShape<T, N, E>::NW * N * sizeof(double);
 }
 
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L>

@@ -231,7 +231,14 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
     constexpr int LPC = NW * LPW;
     constexpr bool kTab = XUsesTable<MODE>::value;
     constexpr uint32_t PSI_BYTES = (uint32_t)(LPC * N * sizeof(cx<T>));
-    constexpr uint32_t BUF_BYTES = kTab ? 2 * PSI_BYTES : PSI_BYTES;
+    // Passes that apply the potential read the x profile of a separable absorber
+    // (N doubles) from shared memory, not between the FFTs from global memory:
+    // batched, each tile buffer carries its instance's profile after the table
+    // rows; one field, the profile is loaded once into the (there unused) slot of
+    // the stage-twiddle copy.
+    constexpr bool kMrowRing = kTab && F::kMany;
+    constexpr uint32_t MROW_BYTES = kMrowRing ? (uint32_t)(N * sizeof(double)) : 0u;
+    constexpr uint32_t BUF_BYTES = kTab ? 2 * PSI_BYTES + MROW_BYTES : PSI_BYTES;
     using S = PlanShape<R0, R1, R2>;
     // batch start: reversed radix order, as the second FFT of the between-steps pass
     constexpr bool kRev = MODE == XM_START;
@@ -253,6 +260,13 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
         fence_mbar_init();
     }
     if (kSmemTw && nmine > 0) TW::load(tws, f.args(blockIdx.x).stw, f.args(blockIdx.x).stwl);
+    static_assert(TW::bytes >= N * sizeof(double), "the absorber profile fits the twiddle slot");
+    double* mrow1 = reinterpret_cast<double*>(tws);  // one field: the absorber's x profile
+    if constexpr (kTab && !F::kMany) {
+        const PassArgs<T>& a0 = f.args(0);
+        if (nmine > 0 && a0.tb.maskfull == nullptr && a0.tb.mask1[0] != nullptr)
+            for (int i = threadIdx.x; i < N; i += blockDim.x) mrow1[i] = a0.tb.mask1[0][i];
+    }
     __syncthreads();
     auto issue = [&](int i) {
         const int buf = i % NBUF;
@@ -265,9 +279,12 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
         const uint32_t bytes = (uint32_t)(nval * N * (int)sizeof(cx<T>));
         const uint32_t bar = smem_u32(&bars[buf]);
         const uint32_t dst = smem_u32(smraw3 + (size_t)buf * BUF_BYTES);
-        mbar_expect_tx(bar, kTab ? 2 * bytes : bytes);
+        const bool sepm = kMrowRing && a.tb.maskfull == nullptr && a.tb.mask1[0] != nullptr;
+        mbar_expect_tx(bar, (kTab ? 2 * bytes : bytes) + (sepm ? MROW_BYTES : 0u));
         bulk_g2s(dst, a.src + m0 * N, bytes, bar);
         if constexpr (kTab) bulk_g2s(dst + PSI_BYTES, vtab + m0 * N, bytes, bar);
+        if constexpr (kMrowRing)
+            if (sepm) bulk_g2s(dst + 2 * PSI_BYTES, a.tb.mask1[0], MROW_BYTES, bar);
     };
     if (threadIdx.x == 0)
         for (int i = 0; i < NBUF && i < nmine; ++i) issue(i);
@@ -292,9 +309,11 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
         // separable absorber: per-line factor my[j] * mz[k] (the mask is m = mx[i] * (my[j] * mz[k]))
         const bool sep = a.tb.maskfull == nullptr && a.tb.mask1[0] != nullptr;
         const double myz = sep ? a.tb.mask1[1][jy] * a.tb.mask1[2][kz] : 1.0;
+        const double* mrow = kMrowRing ? reinterpret_cast<const double*>(smraw3 + (size_t)buf * BUF_BYTES + 2 * PSI_BYTES)
+                                       : mrow1;
         auto mval = [&](int pos) -> double {  // == maskval<T>(a.tb, mc * N + pos, pos, jy, kz)
             if (!sep) return a.tb.maskfull ? a.tb.maskfull[mc * N + pos] : 1.0;
-            return a.tb.mask1[0][pos] * myz;
+            return (kTab ? mrow[pos] : a.tb.mask1[0][pos]) * myz;
         };
         cx<T>* line = ptile + (size_t)lc * N;
         const cx<T>* tline = ttile + (size_t)lc * N;

@@ -33,6 +33,7 @@ struct PlanEntry {
         XBPipe kb[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
         int warps = 0, lpc = 0, nbuf = 0;
         size_t smem[7] = {0, 0, 0, 0, 0, 0, 0};
+        size_t smemb[7] = {0, 0, 0, 0, 0, 0, 0};  // batched forms
         int bps[7] = {0, 0, 0, 0, 0, 0, 0};  // resident CTAs per SM
         int bbps[7] = {0, 0, 0, 0, 0, 0, 0};
     };
@@ -136,12 +137,15 @@ void add_x_variant(PlanEntry<T>& p) {
     }
     for (int m : {XM_FWD, XM_START, XM_MID, XM_END}) {
         v.smem[m] = pipe_tw_offset(NBUF * (m != XM_FWD ? 2 * psi : psi), NBUF) + TwStage<T, R0, R1, R2>::bytes;
+        // batched: each tile buffer also carries its instance's absorber x profile
+        v.smemb[m] = pipe_tw_offset(NBUF * (m != XM_FWD ? 2 * psi + N * sizeof(double) : psi), NBUF) +
+                     TwStage<T, R0, R1, R2>::bytes;
         allow_smem(v.k[m], (int)v.smem[m]);
         cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bps[m], v.k[m], NW * 32, v.smem[m],
                                                               cudaOccupancyDefault);
         if (v.kb[m]) {
-            allow_smem(v.kb[m], (int)v.smem[m]);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bbps[m], v.kb[m], NW * 32, v.smem[m],
+            allow_smem(v.kb[m], (int)v.smemb[m]);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&v.bbps[m], v.kb[m], NW * 32, v.smemb[m],
                                                                   cudaOccupancyDefault);
         }
     }
