@@ -35,6 +35,22 @@ template <typename T>
 __device__ __forceinline__ cx<T> operator-(cx<T> a, cx<T> b) {
     return mk<T>(a.x - b.x, a.y - b.y);
 }
+// complex64 sums and differences as packed FP32 pairs (sm_100 add/sub.f32x2):
+// per component the same IEEE round-to-nearest operation as the scalar form,
+// in one instruction instead of two.
+__device__ __forceinline__ float2 as_f2(cx<float> a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ cx<float> from_f2(float2 a) { return mk<float>(a.x, a.y); }
+__device__ __forceinline__ cx<float> operator+(cx<float> a, cx<float> b) {
+    return from_f2(__fadd2_rn(as_f2(a), as_f2(b)));
+}
+__device__ __forceinline__ cx<float> operator-(cx<float> a, cx<float> b) {
+    cx<float> c;
+    asm("{\n\t.reg .b64 ra, rb, rc;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rc, ra, rb;\n\tmov.b64 {%0, %1}, rc;\n\t}"
+        : "=f"(c.x), "=f"(c.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return c;
+}
 template <typename T>
 __device__ __forceinline__ cx<T> operator*(cx<T> a, cx<T> b) {
     return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -124,6 +140,16 @@ __device__ __forceinline__ T kmul(T a, CK<T> c) {
     else return a * c.hi;
 }
 
+// a * c for complex a and a real compensated constant (componentwise kmul;
+// complex64 as two packed FP32 operations).
+template <typename T>
+__device__ __forceinline__ cx<T> kmulc(cx<T> a, CK<T> c) {
+    if constexpr (sizeof(T) == 4)
+        return from_f2(__ffma2_rn(as_f2(a), make_float2(c.hi, c.hi), __fmul2_rn(as_f2(a), make_float2(c.lo, c.lo))));
+    else
+        return mk<T>(a.x * c.hi, a.y * c.hi);
+}
+
 // v * (c - i s) with compensated constants
 template <typename T>
 __device__ __forceinline__ cx<T> rotc(cx<T> v, CK<T> c, CK<T> s) {
@@ -206,9 +232,12 @@ template <typename T>
 __device__ __forceinline__ void dft3(cx<T>* v) {
     const CK<T> hs3 = ck<T>(0.86602540378443864676);  // sin(2 pi/3)
     const cx<T> t = v[1] + v[2];
-    const cx<T> m = mk<T>(v[0].x - (T)0.5 * t.x, v[0].y - (T)0.5 * t.y);
-    const cx<T> df = v[1] - v[2];
-    const cx<T> d = mk<T>(kmul(df.x, hs3), kmul(df.y, hs3));
+    cx<T> m;  // v0 - t/2 (the halving is exact)
+    if constexpr (sizeof(T) == 4)
+        m = from_f2(__ffma2_rn(as_f2(t), make_float2(-0.5f, -0.5f), as_f2(v[0])));
+    else
+        m = mk<T>(fma(-0.5, t.x, v[0].x), fma(-0.5, t.y, v[0].y));
+    const cx<T> d = kmulc(v[1] - v[2], hs3);
     v[0] = v[0] + t;
     v[1] = mk<T>(m.x + d.y, m.y - d.x);  // m - i d
     v[2] = mk<T>(m.x - d.y, m.y + d.x);  // m + i d
@@ -222,10 +251,10 @@ __device__ __forceinline__ void dft5(cx<T>* v) {
     const CK<T> s2 = ck<T>(0.58778525229247312917);   // sin(4 pi/5)
     const cx<T> a1 = v[1] + v[4], a2 = v[2] + v[3];
     const cx<T> b1 = v[1] - v[4], b2 = v[2] - v[3];
-    const cx<T> p1 = mk<T>(v[0].x + kmul(a1.x, c1) + kmul(a2.x, c2), v[0].y + kmul(a1.y, c1) + kmul(a2.y, c2));
-    const cx<T> p2 = mk<T>(v[0].x + kmul(a1.x, c2) + kmul(a2.x, c1), v[0].y + kmul(a1.y, c2) + kmul(a2.y, c1));
-    const cx<T> q1 = mk<T>(kmul(b1.x, s1) + kmul(b2.x, s2), kmul(b1.y, s1) + kmul(b2.y, s2));
-    const cx<T> q2 = mk<T>(kmul(b1.x, s2) - kmul(b2.x, s1), kmul(b1.y, s2) - kmul(b2.y, s1));
+    const cx<T> p1 = v[0] + kmulc(a1, c1) + kmulc(a2, c2);
+    const cx<T> p2 = v[0] + kmulc(a1, c2) + kmulc(a2, c1);
+    const cx<T> q1 = kmulc(b1, s1) + kmulc(b2, s2);
+    const cx<T> q2 = kmulc(b1, s2) - kmulc(b2, s1);
     v[0] = v[0] + a1 + a2;
     v[1] = mk<T>(p1.x + q1.y, p1.y - q1.x);  // p1 - i q1
     v[4] = mk<T>(p1.x - q1.y, p1.y + q1.x);  // p1 + i q1
