@@ -1,5 +1,5 @@
 // Device building blocks of the split-operator step: complex arithmetic,
-// in-register radix-2/3/4/5/8/16 DFTs, and one Stockham autosort stage over a
+// in-register radix-2/3/4/5/6/8/10/16/20 DFTs, and one Stockham autosort stage over a
 // tile of L lines held in shared memory.
 //
 // The line FFT is the forward unnormalised transform X_k = sum_n x_n e^{-2 pi i kn/N}
@@ -298,6 +298,28 @@ __device__ __forceinline__ void dft10(cx<T>* v) {
     v[9] = a[4] - b[4];
 }
 
+// 20 = 4 x 5 by the same mapping: input n = (5 n1 + 4 n2) mod 20, output
+// k = (5 k1 + 16 k2) mod 20 (5^{-1} = 1 mod 4, 4^{-1} = 4 mod 5).
+template <typename T>
+__device__ __forceinline__ void dft20(cx<T>* v) {
+    cx<T> a[4][5];
+#pragma unroll
+    for (int n2 = 0; n2 < 5; ++n2) {
+        cx<T> c[4];
+#pragma unroll
+        for (int n1 = 0; n1 < 4; ++n1) c[n1] = v[(5 * n1 + 4 * n2) % 20];
+        dft4(c);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) a[k1][n2] = c[k1];
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        dft5(a[k1]);
+#pragma unroll
+        for (int k2 = 0; k2 < 5; ++k2) v[(5 * k1 + 16 * k2) % 20] = a[k1][k2];
+    }
+}
+
 template <typename T, int R>
 __device__ __forceinline__ void dft(cx<T>* v) {
     if constexpr (R == 2) dft2(v);
@@ -308,6 +330,7 @@ __device__ __forceinline__ void dft(cx<T>* v) {
     else if constexpr (R == 8) dft8(v);
     else if constexpr (R == 10) dft10(v);
     else if constexpr (R == 16) dft16(v);
+    else if constexpr (R == 20) dft20(v);
 }
 
 // ---------------------------------------------------------------------------

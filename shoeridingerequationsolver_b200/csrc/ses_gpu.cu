@@ -101,14 +101,16 @@ const Registry& registry() {
     return r;
 }
 
+// The compiled plan of length n for contiguous (kind 1) or strided (kind 2)
+// passes; a length may have a different plan for each kind.
 template <typename T>
-const PlanEntry<T>* find_plan(int n) {
+const PlanEntry<T>* find_plan(int n, int kind) {
     const auto& v = [] () -> const std::vector<PlanEntry<T>>& {
         if constexpr (sizeof(T) == 4) return registry().f;
         else return registry().d;
     }();
     for (const auto& e : v)
-        if (e.n == n) return &e;
+        if (e.n == n && (e.kinds & kind)) return &e;
     return nullptr;
 }
 
@@ -1120,14 +1122,15 @@ void attach_compiled_plan(ses_solver* h, int axis) {
     pp.cp = nullptr;
     if (n < 2) return;
     int e = 0, ls = 0, xw = 4;
+    const int kind = axis == 0 ? 1 : 2;
     if (h->prec == SES_C128) {
-        if (const PlanEntry<double>* p = find_plan<double>(n)) {
+        if (const PlanEntry<double>* p = find_plan<double>(n, kind)) {
             pp.cp = p;
             e = p->e;
             ls = p->ls;
             xw = p->xw;
         }
-    } else if (const PlanEntry<float>* p = find_plan<float>(n)) {
+    } else if (const PlanEntry<float>* p = find_plan<float>(n, kind)) {
         pp.cp = p;
         e = p->e;
         ls = p->ls;
@@ -1275,8 +1278,9 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
             if (ax[0].n % n1) continue;
             const int n2 = ax[0].n / n1;
             if (n2 > n1) continue;
-            const bool ok = prec == SES_C128 ? (find_plan<double>(n1) && find_plan<double>(n2))
-                                             : (find_plan<float>(n1) && find_plan<float>(n2));
+            // N1 runs on the contiguous passes, N2 on the strided ones
+            const bool ok = prec == SES_C128 ? (find_plan<double>(n1, 1) && find_plan<double>(n2, 2))
+                                             : (find_plan<float>(n1, 1) && find_plan<float>(n2, 2));
             if (ok) {
                 long_n1 = n1;
                 long_n2 = n2;

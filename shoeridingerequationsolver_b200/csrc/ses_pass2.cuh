@@ -155,11 +155,12 @@ struct XchWarp {
 // Padding of the contiguous pass's lines: the layouts with the fewest shared-memory
 // wavefronts over every exchange of the plan (forward and reversed orders, both
 // half-warps of 64-bit accesses), found by modelling the access patterns.
-template <int N>
+template <int N, int E>
 struct XPad {
+    static constexpr bool k160e40 = N == 160 && E == 40;  // plan 20 x 8
     static constexpr int SH = N == 160 || N == 96 || N == 64 ? 3 : (N == 48 || N == 32 ? 2 : 4);
     static constexpr int PM = N == 48 ? 3 : 1;
-    static constexpr int LPAD = N == 160 ? 4 : (N == 96 ? 12 : (N == 32 ? 4 : 0));
+    static constexpr int LPAD = k160e40 ? 0 : (N == 160 ? 4 : (N == 96 ? 12 : (N == 32 ? 4 : 0)));
     static constexpr int PITCH = N + PM * (N >> SH) + LPAD;
 };
 
@@ -186,9 +187,12 @@ template <typename T, int N, int E>
 struct XShape {
     static constexpr int TL = N / E;
     static constexpr int LPW = 32 / TL;          // lines per warp
-    static constexpr int PITCH = XPad<N>::PITCH;
+    static constexpr int PITCH = XPad<N, E>::PITCH;
     static constexpr int per_warp = LPW * PITCH * (int)sizeof(cx<T>);
     static constexpr int NW = (48 * 1024) / per_warp >= 4 ? 4 : ((48 * 1024) / per_warp < 1 ? 1 : (48 * 1024) / per_warp);
+    // CTAs per SM the register allocation is sized for: 40 elements per thread
+    // need more than the 128 registers of four 4-warp CTAs
+    static constexpr int MINB = E >= 40 ? 2 : 4;
 };
 
 // Body of the contiguous pass for CTA tile `blk` (NW * LPW lines); `a` is the
@@ -219,7 +223,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
     const long long mc = valid ? m : 0;
     const int kz = (int)fdiv((uint32_t)mc, a.fny);
     const int jy = (int)(mc - (long long)kz * a.ny);
-    XchWarp<T, XPad<N>::SH, XPad<N>::PM> x{xb + (warp * LPW + lw) * PITCH};
+    XchWarp<T, XPad<N, E>::SH, XPad<N, E>::PM> x{xb + (warp * LPW + lw) * PITCH};
     const cx<T>* src = a.src + mc * N;
     cx<T>* dst = a.dst + mc * N;
     cx<T> v[E];
@@ -367,7 +371,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
 }
 
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2>
-__global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4) xpass2_kernel(const PassArgs<T> a) {
+__global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, XShape<T, N, E>::MINB) xpass2_kernel(const PassArgs<T> a) {
     using XS = XShape<T, N, E>;
     __shared__ cx<T> xb[XS::NW * XS::LPW * XS::PITCH];
     xpass2_body<T, MODE, N, E, R0, R1, R2>(a, (long long)blockIdx.x, xb, a.stw, a.stwl);
@@ -547,7 +551,7 @@ struct BatchWork {
 };
 
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2>
-__global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, 4)
+__global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, XShape<T, N, E>::MINB)
     xbatch_kernel(const PassArgs<T>* __restrict__ args, const BatchWork w) {
     using XS = XShape<T, N, E>;
     using TW = TwStage<T, R0, R1, R2>;

@@ -17,6 +17,7 @@ template <typename T>
 struct PlanEntry {
     int n = 0, e = 0, r0 = 1, r1 = 1, r2 = 1;
     int ls = 0;             // lines per strided-pass CTA
+    int kinds = 3;          // passes this entry serves: 1 contiguous (x), 2 strided (y, z)
     int xw = 4;             // warps per contiguous-pass CTA
     size_t twb = 0;         // bytes of the shared-memory stage-twiddle copy (persistent kernels)
     size_t xbsm = 0;        // dynamic shared memory of the batched register-path x pass

@@ -1,5 +1,6 @@
 // Compiled plans with radix-3/5 factors: 48 = 4x4x3, 96 = 6x4x4, 160 = 10x4x4
-// (radix 6 and 10 are prime-factor butterflies), with pipelined complex64 variants.
+// (complex64 strided passes: 20x8); radix 6, 10 and 20 are prime-factor
+// butterflies.  Pipelined complex64 variants.
 #include "ses_plans.cuh"
 
 namespace sesk {
@@ -15,11 +16,18 @@ void register_plans_mixed(std::vector<PlanEntry<float>>& f, std::vector<PlanEntr
     add_s_variant<float, 96, 12, 6, 4, 4, 32, 2, 2>(f.back());
     add_s_variant<float, 96, 12, 6, 4, 4, 16, 2, 4>(f.back());
     d.push_back(make_plan_entry<double, 96, 12, 6, 4, 4, 16>());
+    // complex64 160: the contiguous passes keep 10 x 4 x 4 (20 elements per
+    // thread, 16 warps per SM); the strided passes run 20 x 8 with 40 elements
+    // per thread -- one exchange and one twiddled stage per transform, where
+    // the tile in shared memory, not the registers, limits the warps per SM.
     f.push_back(make_plan_entry<float, 160, 20, 10, 4, 4, 32>());
+    f.back().kinds = 1;
     add_x_variant<float, 160, 20, 10, 4, 4, 4, 2, 2>(f.back());
     add_x_variant<float, 160, 20, 10, 4, 4, 2, 2, 4>(f.back());
-    add_s_variant<float, 160, 20, 10, 4, 4, 32, 2, 2>(f.back());
-    add_s_variant<float, 160, 20, 10, 4, 4, 16, 2, 4>(f.back());
+    f.push_back(make_plan_entry<float, 160, 40, 20, 8, 1, 32>());
+    f.back().kinds = 2;
+    add_s_variant<float, 160, 40, 20, 8, 1, 32, 2, 2>(f.back());
+    add_s_variant<float, 160, 40, 20, 8, 1, 16, 2, 4>(f.back());
     d.push_back(make_plan_entry<double, 160, 20, 10, 4, 4, 16>());
 }
 }  // namespace sesk

@@ -203,16 +203,17 @@ def test_plans_stay_in_bounds(dims, es):
 # fused passes -- modelled exactly and compared with numpy's FFT.
 
 COMPILED_PLANS = [(16, 16, (16,)), (32, 8, (8, 4)), (48, 12, (4, 4, 3)), (64, 8, (8, 8)),
-                  (96, 12, (6, 4, 4)), (128, 16, (16, 8)), (160, 20, (10, 4, 4)), (256, 16, (16, 16)),
+                  (96, 12, (6, 4, 4)), (128, 16, (16, 8)), (160, 20, (10, 4, 4)), (160, 40, (20, 8)),
+                  (256, 16, (16, 16)),
                   (512, 16, (8, 8, 8)), (1024, 32, (16, 8, 8))]
 
 
-def xpad(N):
+def xpad(N, E):
     """Contiguous-pass line padding (ses_pass2.cuh XPad): element pos at pos + PM (pos >> SH),
     line pitch N + PM (N >> SH) + LPAD."""
     sh = 3 if N in (160, 96, 64) else (2 if N in (48, 32) else 4)
     pm = 3 if N == 48 else 1
-    lpad = {160: 4, 96: 12, 32: 4}.get(N, 0)
+    lpad = 0 if (N, E) == (160, 40) else {160: 4, 96: 12, 32: 4}.get(N, 0)
     return sh, pm, lpad
 
 
@@ -255,7 +256,7 @@ def model_fft(x, N, E, rads, tab, toff):
                     for r in range(R):
                         pos = (j - k) * R + k + r * Ns
                         assert 0 <= pos < N and np.isnan(buf[pos])  # each slot written once
-                        sh, pm, _ = xpad(N)
+                        sh, pm, _ = xpad(N, E)
                         smem_max = max(smem_max, pos + pm * (pos >> sh))
                         buf[pos] = v[q][b * R + r]
             v = [[buf[q + TL * b + r * (N // Rn)] for b in range(E // Rn) for r in range(Rn)]
@@ -268,7 +269,7 @@ def model_fft(x, N, E, rads, tab, toff):
         for b in range(E // RL):
             for r in range(RL):
                 out[q + TL * b + r * (N // RL)] = v[q][b * RL + r]
-    sh, pm, lpad = xpad(N)
+    sh, pm, lpad = xpad(N, E)
     assert smem_max < N + pm * (N >> sh) + lpad or len(rads) == 1
     return out
 
