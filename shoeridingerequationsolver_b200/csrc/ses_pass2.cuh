@@ -193,6 +193,16 @@ struct XShape {
     // CTAs per SM the register allocation is sized for: 40 elements per thread
     // need more than the 128 registers of four 4-warp CTAs
     static constexpr int MINB = E >= 40 ? 2 : 4;
+    // Pitch of the staged potential-table rows of the batched pass: a
+    // half-warp reads 16/TL lines at the same positions, each line covering 2 TL
+    // banks with 64-bit elements; a pitch of TL mod 16 puts those lines on
+    // disjoint banks (a pitch of N, a multiple of 16, puts them on the same).
+    // The pitch stays even: rows are filled by 16-byte cp.async copies, whose
+    // shared-memory address must be 16-byte aligned (one thread per line, TL = 1,
+    // takes pitch 2 mod 16 instead of 1).
+    static constexpr int RTL = TL < 2 ? 2 : TL;
+    static constexpr int RPITCH = TL >= 16 ? N : N + ((RTL - N % 16) % 16 + 16) % 16;
+    static_assert(RPITCH % 2 == 0, "staged rows start on 16-byte boundaries");
 };
 
 // Body of the contiguous pass for CTA tile `blk` (NW * LPW lines); `a` is the
@@ -228,12 +238,27 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
     cx<T>* dst = a.dst + mc * N;
     cx<T> v[E];
     constexpr bool kTabLate = MODE == XM_MID || MODE == XM_END;  // table used after the first FFT
-    cx<T>* vrow = vt ? vt + (size_t)(warp * LPW + lw) * N : nullptr;
+    constexpr int RP = XS::RPITCH;
+    cx<T>* vrow = vt ? vt + (size_t)(warp * LPW + lw) * RP : nullptr;
     const double* mfull = a.tb.maskfull;
     const double* mx = a.tb.mask1[0];
     // this warp's copy of the x profile of a separable absorber (N doubles after the
     // table rows of all warps), staged with the rows by the passes that use it
-    double* ms = vt ? reinterpret_cast<double*>(vt + (size_t)NW * LPW * N) + (size_t)warp * N : nullptr;
+    double* ms = vt ? reinterpret_cast<double*>(vt + (size_t)NW * LPW * RP) + (size_t)warp * N : nullptr;
+    // load the first FFT's inputs (coalesced along the line)
+    constexpr bool kConjIn = MODE == XM_INV || MODE == XM_MID || MODE == XM_END;
+#pragma unroll
+    for (int b = 0; b < E / RF; ++b)
+#pragma unroll
+        for (int r = 0; r < RF; ++r) {
+            const int pos = q + TL * b + r * (N / RF);
+            cx<T> e = valid ? src[pos] : czero<T>();
+            if constexpr (MODE == XM_START || MODE == XM_1D) {
+                if (a.d_load != DG_NONE || a.m_load)
+                    e = apply_diag(e, a.d_load, a.m_load, mc * N + pos, pos, jy, kz, a.tb);
+            }
+            v[b * RF + r] = kConjIn ? cconj(e) : e;
+        }
     if constexpr (kTabLate) {
         const bool want = MODE == XM_MID ? a.d_mid != DG_NONE : a.d_store != DG_NONE;
         const bool wantm = (MODE == XM_MID ? a.m_mid : a.m_store) && !mfull && mx;
@@ -246,7 +271,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
                 for (int c = lane; c < LPW * CH; c += 32) {
                     const int ln = c / CH, ch = c - ln * CH;
                     if (m0 + ln < a.nlines)
-                        cp_async16(reinterpret_cast<char*>(vt + (size_t)(warp * LPW + ln) * N) + 16 * ch,
+                        cp_async16(reinterpret_cast<char*>(vt + (size_t)(warp * LPW + ln) * RP) + 16 * ch,
                                    reinterpret_cast<const char*>(tab + (m0 + ln) * N) + 16 * ch);
                 }
             }
@@ -270,21 +295,6 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
         }
         return apply_diag(e, kind, msk, f, pos, jy, kz, a.tb);
     };
-
-    // load the first FFT's inputs (coalesced along the line)
-    constexpr bool kConjIn = MODE == XM_INV || MODE == XM_MID || MODE == XM_END;
-#pragma unroll
-    for (int b = 0; b < E / RF; ++b)
-#pragma unroll
-        for (int r = 0; r < RF; ++r) {
-            const int pos = q + TL * b + r * (N / RF);
-            cx<T> e = valid ? src[pos] : czero<T>();
-            if constexpr (MODE == XM_START || MODE == XM_1D) {
-                if (a.d_load != DG_NONE || a.m_load)
-                    e = apply_diag(e, a.d_load, a.m_load, mc * N + pos, pos, jy, kz, a.tb);
-            }
-            v[b * RF + r] = kConjIn ? cconj(e) : e;
-        }
 
     rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, twh, twl, x);
     // v[b*RL + r] now at position q + TL b + r N/RL
@@ -568,11 +578,11 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, XShape<T, N, E>::MIN
 }
 
 // Dynamic shared memory of xbatch_kernel: stage twiddles, then NW * LPW table
-// rows, then one x profile of the absorber (N doubles) per warp.
+// rows (pitch RPITCH), then one x profile of the absorber (N doubles) per warp.
 template <typename T, int N, int E, int R0, int R1, int R2>
 constexpr size_t xbatch_smem() {
     return TwStage<T, R0, R1, R2>::bytes +
-           (size_t)XShape<T, N, E>::NW * XShape<T, N, E>::LPW * N * sizeof(cx<T>) +
+           (size_t)XShape<T, N, E>::NW * XShape<T, N, E>::LPW * XShape<T, N, E>::RPITCH * sizeof(cx<T>) +
            (size_t)XShape<T, N, E>::NW * N * sizeof(double);
 }
 
