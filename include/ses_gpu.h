@@ -253,6 +253,22 @@ SES_API ses_status ses_batch_step(ses_batch b, int nsteps, int absorb);
 /* ses_gpu_observe of every member, in the order they were added (count must be
  * the member count), with one wait for the whole batch. */
 SES_API ses_status ses_batch_observe(ses_batch b, double xlo, double xhi, ses_observables* out, int count);
+/* One round trip of every member with host buffers, as upload_state -> step
+ * batch -> observables -> readback of the reference Engine (vk_engine.ixx:
+ * 1083-1089, 597-698, 2136-2155) for each instance: psi_in[i] / psi_out[i]
+ * are interleaved complex128 host arrays of member i (null entries skip that
+ * member's upload or readback; null arrays skip all), obs (nullable) receives
+ * ses_gpu_observe(xlo, xhi) after the steps, members in the order they were
+ * added (count must be the member count).  Each class's uploads, steps,
+ * observables and readbacks are queued on its own stream, largest class
+ * first, so one class's PCIe transfers overlap the other classes' steps; the
+ * results equal write_psi + ses_batch_step + observe + read_psi.  Host arrays
+ * should be page-locked (cudaHostAlloc / pinned tensors): pageable memory
+ * works but its copies do not overlap.  Blocks until done or timeout_ms
+ * (<= 0: 60 s) has passed (SES_ETIMEDOUT). */
+SES_API ses_status ses_batch_run(ses_batch b, const double* const* psi_in, int nsteps, int absorb, double xlo,
+                                 double xhi, ses_observables* obs, double* const* psi_out, int count,
+                                 int timeout_ms);
 /* The same for the listed members only, each with its own x-interval. */
 SES_API ses_status ses_batch_observe_some(ses_batch b, const ses_handle* hs, int count, const double* xlo,
                                           const double* xhi, ses_observables* out);

@@ -29,7 +29,7 @@ EXPORTS = [
     "ses_serve_open", "ses_serve_submit", "ses_serve_poll", "ses_serve_result", "ses_serve_cancel",
     "ses_serve_wait_idle", "ses_serve_stats", "ses_serve_close", "ses_gpu_create_imag", "ses_gpu_relax",
     "ses_gpu_step_driven", "ses_gpu_snapshot", "ses_gpu_restore", "ses_gpu_density_slice",
-    "ses_batch_observe_some",
+    "ses_batch_observe_some", "ses_batch_run",
 ]
 
 
@@ -136,6 +136,8 @@ def _load() -> C.CDLL:
         "ses_batch_observe": ([vp, C.c_double, C.c_double, C.POINTER(Observables), C.c_int], st),
         "ses_batch_sync": ([vp, C.c_int], st),
         "ses_batch_observe_some": ([vp, C.POINTER(hp), C.c_int, dp, dp, C.POINTER(Observables)], st),
+        "ses_batch_run": ([vp, C.POINTER(dp), C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(Observables),
+                           C.POINTER(dp), C.c_int, C.c_int], st),
         "ses_batch_set_stream": ([vp, vp], st),
         "ses_batch_members": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], st),
         "ses_batch_profile": ([vp, C.c_int, C.c_int, dp, C.c_int], st),

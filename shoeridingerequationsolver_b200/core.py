@@ -488,6 +488,44 @@ class Batch:
     def sync(self, timeout_ms: int = 0) -> None:
         check(lib.ses_batch_sync(self._b, int(timeout_ms)))
 
+    def run(self, nsteps: int, psi_in=None, psi_out=None, absorb: bool = False,
+            xlo: float = -math.inf, xhi: float = math.inf, observe: bool = True,
+            timeout_ms: int = 0):
+        """One host round trip of every member (ses_batch_run): upload psi_in[i]
+        (or skip where None), nsteps steps, observables, read back into psi_out[i].
+        Entries are contiguous complex128 numpy arrays of the member's size or raw
+        host addresses (ints) of such arrays; page-locked memory lets each class's
+        transfers overlap the other classes' steps.  Returns the observables (a
+        list of dicts, member order) or None."""
+        n = len(self._members)
+
+        def ptrs(seq, name):
+            if seq is None:
+                return None
+            if len(seq) != n:
+                raise ValueError(f"{name} needs one entry per member ({n})")
+            arr = (C.POINTER(C.c_double) * max(n, 1))()
+            for i, (x, op) in enumerate(zip(seq, self._members)):
+                if x is None:
+                    continue
+                if isinstance(x, int):
+                    addr = x
+                else:
+                    if not (isinstance(x, np.ndarray) and x.dtype == np.complex128 and x.flags.c_contiguous
+                            and x.size == op.grid.size()):
+                        raise ValueError(f"{name}[{i}] must be a contiguous complex128 array of the member's size")
+                    if name == "psi_out" and not x.flags.writeable:
+                        raise ValueError("psi_out arrays must be writeable")
+                    addr = x.ctypes.data
+                arr[i] = C.cast(C.c_void_p(addr), C.POINTER(C.c_double))
+            return arr
+
+        pin, pout = ptrs(psi_in, "psi_in"), ptrs(psi_out, "psi_out")
+        out = (_abi.Observables * max(n, 1))() if observe else None
+        check(lib.ses_batch_run(self._b, pin, int(nsteps), 1 if absorb else 0, float(xlo), float(xhi),
+                                out, pout, n, int(timeout_ms)))
+        return [out[i].as_dict() for i in range(n)] if observe else None
+
     def set_stream(self, stream_ptr: int | None) -> None:
         check(lib.ses_batch_set_stream(self._b, C.c_void_p(stream_ptr or 0)))
 

@@ -2028,6 +2028,47 @@ ses_status batch_remove_impl(ses_batch_s* b, ses_solver* h) {
 
 }  // namespace
 
+// Host <-> device copies of one field on stream s, queued without waiting:
+// complex128 directly; complex64 staged in halves through the scratch field
+// (rounded on upload, widened on readback).
+ses_status enqueue_write_psi(ses_solver* h, const double* psi_in, cudaStream_t s) {
+    const size_t N = (size_t)h->N;
+    if (h->prec == SES_C128) {
+        SES_CU(cudaMemcpyAsync(h->psi, psi_in, N * 16, cudaMemcpyHostToDevice, s));
+        return SES_OK;
+    }
+    const size_t half = (N + 1) / 2;
+    for (size_t off = 0; off < N; off += half) {
+        const size_t cnt = std::min(half, N - off);
+        SES_CU(cudaMemcpyAsync(h->scratch, psi_in + 2 * off, cnt * 16, cudaMemcpyHostToDevice, s));
+        const unsigned gb = (unsigned)std::min<size_t>((cnt + 255) / 256, 148 * 32);
+        convert_kernel<double, float><<<gb, 256, 0, s>>>(reinterpret_cast<const cx<double>*>(h->scratch),
+                                                          reinterpret_cast<cx<float>*>(h->psi) + off,
+                                                          (long long)cnt);
+        SES_CU(cudaGetLastError());
+    }
+    return SES_OK;
+}
+
+ses_status enqueue_read_psi(ses_solver* h, double* psi_out, cudaStream_t s) {
+    const size_t N = (size_t)h->N;
+    if (h->prec == SES_C128) {
+        SES_CU(cudaMemcpyAsync(psi_out, h->psi, N * 16, cudaMemcpyDeviceToHost, s));
+        return SES_OK;
+    }
+    const size_t half = (N + 1) / 2;
+    for (size_t off = 0; off < N; off += half) {
+        const size_t cnt = std::min(half, N - off);
+        const unsigned gb = (unsigned)std::min<size_t>((cnt + 255) / 256, 148 * 32);
+        convert_kernel<float, double><<<gb, 256, 0, s>>>(reinterpret_cast<const cx<float>*>(h->psi) + off,
+                                                          reinterpret_cast<cx<double>*>(h->scratch),
+                                                          (long long)cnt);
+        SES_CU(cudaGetLastError());
+        SES_CU(cudaMemcpyAsync(psi_out + 2 * off, h->scratch, cnt * 16, cudaMemcpyDeviceToHost, s));
+    }
+    return SES_OK;
+}
+
 extern "C" {
 
 const char* ses_version(void) { return "ses-b200 0.1 (sm_100a)"; }
@@ -2250,43 +2291,14 @@ ses_status ses_gpu_observe(ses_handle h, double xlo, double xhi, ses_observables
 ses_status ses_gpu_write_psi(ses_handle h, const double* psi_in) {
     SES_TRY(check_handle(h));
     if (!psi_in) return fail(SES_EINVAL, "null psi");
-    const size_t N = (size_t)h->N;
-    if (h->prec == SES_C128) {
-        SES_CU(cudaMemcpyAsync(h->psi, psi_in, N * 16, cudaMemcpyHostToDevice, h->stream));
-        return wait_bounded(h, 0);
-    }
-    // C64: stage complex128 halves through the scratch field, round on device
-    const size_t half = (N + 1) / 2;
-    for (size_t off = 0; off < N; off += half) {
-        const size_t cnt = std::min(half, N - off);
-        SES_CU(cudaMemcpyAsync(h->scratch, psi_in + 2 * off, cnt * 16, cudaMemcpyHostToDevice, h->stream));
-        const unsigned gb = (unsigned)std::min<size_t>((cnt + 255) / 256, 148 * 32);
-        convert_kernel<double, float><<<gb, 256, 0, h->stream>>>(
-            reinterpret_cast<const cx<double>*>(h->scratch), reinterpret_cast<cx<float>*>(h->psi) + off,
-            (long long)cnt);
-        SES_CU(cudaGetLastError());
-    }
+    SES_TRY(enqueue_write_psi(h, psi_in, h->stream));
     return wait_bounded(h, 0);
 }
 
 ses_status ses_gpu_read_psi(ses_handle h, double* psi_out) {
     SES_TRY(check_handle(h));
     if (!psi_out) return fail(SES_EINVAL, "null psi");
-    const size_t N = (size_t)h->N;
-    if (h->prec == SES_C128) {
-        SES_CU(cudaMemcpyAsync(psi_out, h->psi, N * 16, cudaMemcpyDeviceToHost, h->stream));
-        return wait_bounded(h, 0);
-    }
-    const size_t half = (N + 1) / 2;
-    for (size_t off = 0; off < N; off += half) {
-        const size_t cnt = std::min(half, N - off);
-        const unsigned gb = (unsigned)std::min<size_t>((cnt + 255) / 256, 148 * 32);
-        convert_kernel<float, double><<<gb, 256, 0, h->stream>>>(
-            reinterpret_cast<const cx<float>*>(h->psi) + off, reinterpret_cast<cx<double>*>(h->scratch),
-            (long long)cnt);
-        SES_CU(cudaGetLastError());
-        SES_CU(cudaMemcpyAsync(psi_out + 2 * off, h->scratch, cnt * 16, cudaMemcpyDeviceToHost, h->stream));
-    }
+    SES_TRY(enqueue_read_psi(h, psi_out, h->stream));
     return wait_bounded(h, 0);
 }
 
@@ -2548,6 +2560,62 @@ ses_status ses_batch_observe(ses_batch b, double xlo, double xhi, ses_observable
         SES_TRY(h->prec == SES_C128 ? enqueue_observe<double>(h, xlo, xhi) : enqueue_observe<float>(h, xlo, xhi));
     SES_TRY(batch_wait(b, 0));
     for (int i = 0; i < count; ++i) finish_observe(b->members[i], &out[i]);
+    return SES_OK;
+}
+
+ses_status ses_batch_run(ses_batch b, const double* const* psi_in, int nsteps, int absorb, double xlo,
+                         double xhi, ses_observables* obs, double* const* psi_out, int count, int timeout_ms) {
+    SES_TRY(check_batch(b));
+    if (nsteps < 0) return fail(SES_EINVAL, "nsteps must be >= 0");
+    if (count != (int)b->members.size())
+        return fail(SES_EINVAL, "count must equal the number of members (" +
+                                    std::to_string(b->members.size()) + ")");
+    SES_TRY(batch_refresh(b));
+    std::map<const ses_solver*, int> index;
+    for (int i = 0; i < count; ++i) index[b->members[i]] = i;
+    // largest class first: its steps start while the others are still uploading
+    std::vector<BatchClass*> order(b->classes.begin(), b->classes.end());
+    std::stable_sort(order.begin(), order.end(), [](const BatchClass* x, const BatchClass* y) {
+        return (double)x->mem.size() * x->n[0] * x->n[1] * x->n[2] > (double)y->mem.size() * y->n[0] * y->n[1] * y->n[2];
+    });
+    const bool mask = absorb != 0;
+    SES_CU(cudaEventRecord(b->fork, b->stream));
+    for (BatchClass* c : order) {
+        if (c->mem.empty()) continue;
+        const cudaStream_t s = c->batched ? c->cs : b->stream;
+        if (c->batched) SES_CU(cudaStreamWaitEvent(s, b->fork, 0));
+        for (ses_solver* h : c->mem) h->stream = s;  // the member-level enqueues below go to s
+        auto queue = [&]() -> ses_status {
+            if (psi_in)
+                for (ses_solver* h : c->mem)
+                    if (const double* p = psi_in[index[h]]) SES_TRY(enqueue_write_psi(h, p, s));
+            if (nsteps > 0) {
+                if (c->batched)
+                    SES_TRY(c->prec == SES_C128 ? class_steps<double>(b, *c, nsteps, mask, s)
+                                                : class_steps<float>(b, *c, nsteps, mask, s));
+                else
+                    for (ses_solver* h : c->mem) SES_TRY(ses_gpu_step(h, nsteps, absorb));
+            }
+            if (obs)
+                for (ses_solver* h : c->mem)
+                    SES_TRY(h->prec == SES_C128 ? enqueue_observe<double>(h, xlo, xhi)
+                                                : enqueue_observe<float>(h, xlo, xhi));
+            if (psi_out)
+                for (ses_solver* h : c->mem)
+                    if (double* p = psi_out[index[h]]) SES_TRY(enqueue_read_psi(h, p, s));
+            return SES_OK;
+        };
+        const ses_status st = queue();
+        for (ses_solver* h : c->mem) h->stream = b->stream;
+        if (c->batched) {
+            SES_CU(cudaEventRecord(c->done, s));
+            SES_CU(cudaStreamWaitEvent(b->stream, c->done, 0));
+        }
+        if (st != SES_OK) return st;
+    }
+    SES_TRY(batch_wait(b, timeout_ms > 0 ? timeout_ms : 60000));
+    if (obs)
+        for (int i = 0; i < count; ++i) finish_observe(b->members[i], &obs[i]);
     return SES_OK;
 }
 

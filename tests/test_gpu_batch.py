@@ -137,3 +137,50 @@ def test_batch_profile_reports_every_class(ses):
             assert 0.5 < o["norm"] <= 1.0 + 1e-6
     for op in ops:
         op.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+def test_batch_run_equals_separate_calls(ses, prec):
+    """ses_batch_run (uploads, steps, observables and readbacks queued per class
+    stream) gives the bits of write_psi + ses_batch_step + observe + read_psi on
+    twin members; members without an input keep their field, members without an
+    output are not read back."""
+    box = (8.0, 7.0, 6.0)
+    shapes = [(64, 64, 64), (48, 48, 48), (96, 96, 1), (32, 16, 48), (64, 64, 64), (128, 1, 1)]
+    run_ops, sep_ops, inputs = [], [], []
+    for i, shape in enumerate(shapes):
+        a, _ = make_member(ses, shape, box, prec, seed=300 + i)
+        b, _ = make_member(ses, shape, box, prec, seed=300 + i)
+        rng = np.random.default_rng(900 + i)
+        g = a.grid
+        c = [float(rng.uniform(-0.2, 0.2)) * box[k] if shape[k] > 1 else 0.0 for k in range(3)]
+        psi = scenes.gaussian(g, c, [max(0.15 * box[k], 0.3) for k in range(3)],
+                              [float(rng.uniform(-1, 1)) if shape[k] > 1 else 0.0 for k in range(3)])
+        run_ops.append(a)
+        sep_ops.append(b)
+        inputs.append(None if i == 2 else np.ascontiguousarray(psi))
+    outputs = [None if i == 3 else np.full(op.grid.size(), np.nan, complex) for i, op in enumerate(run_ops)]
+    with ses.Batch(run_ops) as br, ses.Batch(sep_ops) as bs:
+        obs_run = br.run(7, psi_in=inputs, psi_out=outputs, absorb=True, xlo=0.0, xhi=math.inf)
+        for op, x in zip(sep_ops, inputs):
+            if x is not None:
+                op.upload_state(x)
+        bs.step(7, absorb=True)
+        obs_sep = bs.observe(0.0, math.inf)
+        for i, (a, b) in enumerate(zip(run_ops, sep_ops)):
+            want = b.readback()
+            if outputs[i] is not None:
+                assert np.array_equal(outputs[i], want), shapes[i]
+            assert np.array_equal(a.readback(), want), shapes[i]
+            assert obs_run[i] == obs_sep[i], shapes[i]
+        # a second round trip on the same buffers: steps only, no observables
+        assert br.run(3, psi_out=outputs, absorb=True, observe=False) is None
+        bs.step(3, absorb=True)
+        for i, b in enumerate(sep_ops):
+            if outputs[i] is not None:
+                assert np.array_equal(outputs[i], b.readback()), shapes[i]
+        with pytest.raises(ValueError):
+            br.run(1, psi_in=inputs[:2])
+    for op in run_ops + sep_ops:
+        op.close()
