@@ -126,19 +126,12 @@ void push_record(ses_server_s* s, Request& r, const ses_observables& o, bool fin
     r.records.push_back(rec);
 }
 
-// Leave the batch, free the device memory, publish the final state (worker thread).
-void retire(ses_server_s* s, const std::shared_ptr<Request>& r, int state, const std::string& err) {
-    if (r->h) {
-        ses_batch_remove(s->batch, r->h);
-        ses_gpu_destroy(r->h);
-        r->h = nullptr;
-    }
-    s->used -= std::min(s->used, r->bytes);
+// Publish a request's final state (worker thread); its handle is released by the caller.
+void publish(ses_server_s* s, const std::shared_ptr<Request>& r, int state, const std::string& err) {
     std::lock_guard<std::mutex> lk(s->mu);
     r->state = state;
     r->error = err;
     --s->running;
-    s->used_view = s->used;
     if (state == SES_REQ_DONE) {
         r->latency_ms = ms_since(r->t_submit);
         s->latencies.push_back(r->latency_ms);
@@ -150,23 +143,39 @@ void retire(ses_server_s* s, const std::shared_ptr<Request>& r, int state, const
     }
 }
 
-// Create the handle of a queued request and add it to the batch (worker
-// thread).  Returns false when the device is out of memory (retry later).
-bool admit_one(ses_server_s* s, const std::shared_ptr<Request>& r) {
+// Free a request's device memory (leaving the batch first if it is a member).
+void release_handle(ses_server_s* s, const std::shared_ptr<Request>& r) {
+    if (r->h) {
+        ses_gpu_destroy(r->h);  // removes it from the batch when it is a member
+        r->h = nullptr;
+    }
+    s->used -= std::min(s->used, r->bytes);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->used_view = s->used;
+}
+
+void retire(ses_server_s* s, const std::shared_ptr<Request>& r, int state, const std::string& err) {
+    release_handle(s, r);
+    publish(s, r, state, err);
+}
+
+// Create the handle of a queued request (worker thread); it joins the batch
+// later, between rounds.  0: created; 1: out of device memory while other
+// requests hold memory (retry later); 2: failed and published.
+int create_one(ses_server_s* s, const std::shared_ptr<Request>& r, bool others_hold_memory) {
     ses_handle h = nullptr;
     ses_status st = ses_gpu_create(&r->grid, r->prec, r->dt, r->mass, r->V.data(), r->psi0.data(), &h);
     if (st == SES_OK && !r->mx.empty())
         st = ses_gpu_set_absorber_separable(h, r->mx.data(), r->my.data(), r->mz.data());
-    if (st == SES_OK) st = ses_batch_add(s->batch, h);
     if (st != SES_OK) {
         const std::string err = ses_last_error();
         if (h) ses_gpu_destroy(h);
-        if (st == SES_ENOMEM && !s->active.empty()) return false;
+        if (st == SES_ENOMEM && others_hold_memory) return 1;
         std::lock_guard<std::mutex> lk(s->mu);
         r->state = SES_REQ_FAILED;
         r->error = err;
         ++s->failed;
-        return true;
+        return 2;
     }
     size_t b = 0;
     ses_gpu_footprint(h, &b);
@@ -175,29 +184,43 @@ bool admit_one(ses_server_s* s, const std::shared_ptr<Request>& r) {
     s->used += r->bytes;
     r->V = std::vector<double>();
     r->psi0 = std::vector<double>();
-    {
-        std::lock_guard<std::mutex> lk(s->mu);
-        r->state = SES_REQ_RUNNING;
-        ++s->admitted;
-        ++s->running;
-        s->used_view = s->used;
-    }
-    s->active.push_back(r);
-    return true;
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->state = SES_REQ_RUNNING;
+    ++s->admitted;
+    ++s->running;
+    s->used_view = s->used;
+    return 0;
 }
 
+// The worker: rounds run asynchronously on the batch stream while the host
+// admits new requests (creates their handles and tables) and reads back the
+// fields of requests that finished in the previous round; handles are freed
+// only between rounds (freeing device memory waits for the device).
 void worker_main(ses_server_s* s) {
     cudaSetDevice(s->dev);
+    std::vector<std::shared_ptr<Request>> pending;    // created, join the batch before the next round
+    std::vector<std::shared_ptr<Request>> finishing;  // left the batch, field still to read back
+    std::vector<std::shared_ptr<Request>> zombies;    // read back, handle to free between rounds
+    bool inflight = false;
+    int R = 0;
+    Clock::time_point t_round;
+    auto fail_active = [&](const std::string& err) {
+        for (const auto& r : s->active) retire(s, r, SES_REQ_FAILED, err);
+        s->active.clear();
+    };
     for (;;) {
-        // admission: first come, first served, while the estimate fits the budget
+        // 1. admission, first come first served while the estimate fits the budget
+        //    (overlaps the round in flight)
         std::vector<std::shared_ptr<Request>> take;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            if (s->active.empty() && s->queue.empty()) {
+            if (!inflight && s->active.empty() && pending.empty() && finishing.empty() && s->queue.empty()) {
                 s->idle.notify_all();
                 s->cv.wait(lk, [&] { return s->stop || !s->queue.empty(); });
             }
-            if (s->stop && s->queue.empty() && s->active.empty()) break;
+            if (s->stop && s->queue.empty() && s->active.empty() && pending.empty() && !inflight &&
+                finishing.empty())
+                break;
             size_t room = s->budget > s->used ? s->budget - s->used : 0;
             while (!s->queue.empty()) {
                 std::shared_ptr<Request> r = s->queue.front();
@@ -214,13 +237,77 @@ void worker_main(ses_server_s* s) {
                 s->queue.pop_front();
             }
         }
-        for (size_t i = 0; i < take.size(); ++i)
-            if (!admit_one(s, take[i])) {  // out of device memory: back to the head of the queue
+        for (size_t i = 0; i < take.size(); ++i) {
+            const bool others = inflight || !s->active.empty() || !pending.empty() || !zombies.empty();
+            const int c = create_one(s, take[i], others);
+            if (c == 0) pending.push_back(take[i]);
+            if (c == 1) {  // out of device memory: back to the head of the queue
                 std::lock_guard<std::mutex> lk(s->mu);
                 for (size_t j = take.size(); j-- > i;) s->queue.push_front(take[j]);
                 break;
             }
-        // cancellations of running requests
+        }
+
+        // 2. the round in flight: wait, free what finished before it, observe, collect finished
+        if (inflight) {
+            ses_status st = ses_batch_sync(s->batch, 600000);
+            inflight = false;
+            const double round_ms = ms_since(t_round);
+            for (const auto& r : zombies) release_handle(s, r);
+            zombies.clear();
+            if (st != SES_OK) {
+                fail_active(ses_last_error());
+            } else {
+                double pts = 0;
+                for (const auto& r : s->active) pts += (double)grid_points(r->grid) * R;
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    ++s->rounds;
+                    s->gridpt_steps += pts;
+                    s->busy_ms += round_ms;
+                }
+                std::vector<ses_handle> oh;
+                std::vector<double> olo, ohi;
+                std::vector<size_t> oi;
+                for (size_t i = 0; i < s->active.size(); ++i) {
+                    Request& r = *s->active[i];
+                    r.done += R;
+                    if (r.done >= r.nsteps || (r.every > 0 && r.done % r.every == 0)) {
+                        oh.push_back(r.h);
+                        olo.push_back(r.xlo);
+                        ohi.push_back(r.xhi);
+                        oi.push_back(i);
+                    }
+                }
+                std::vector<ses_observables> obs(oh.size());
+                if (!oh.empty())
+                    st = ses_batch_observe_some(s->batch, oh.data(), (int)oh.size(), olo.data(), ohi.data(),
+                                                obs.data());
+                if (st != SES_OK) {
+                    fail_active(ses_last_error());
+                } else {
+                    for (size_t q = 0; q < oi.size(); ++q) {
+                        Request& r = *s->active[oi[q]];
+                        push_record(s, r, obs[q], r.done >= r.nsteps);
+                    }
+                    for (size_t i = 0; i < s->active.size();) {
+                        std::shared_ptr<Request> r = s->active[i];
+                        if (r->done >= r->nsteps) {
+                            ses_batch_remove(s->batch, r->h);  // its own stream from now on
+                            finishing.push_back(r);
+                            s->active.erase(s->active.begin() + (long)i);
+                            continue;
+                        }
+                        ++i;
+                    }
+                }
+            }
+        } else {
+            for (const auto& r : zombies) release_handle(s, r);
+            zombies.clear();
+        }
+
+        // 3. cancellations of running requests (no round in flight)
         for (size_t i = 0; i < s->active.size();) {
             bool c;
             {
@@ -234,78 +321,64 @@ void worker_main(ses_server_s* s) {
                 ++i;
             }
         }
-        if (s->active.empty()) {
-            std::this_thread::sleep_for(std::chrono::microseconds(200));
-            continue;
-        }
 
-        // one round: up to the earliest observation point or completion of any member
-        int R = s->max_round;
-        for (const auto& r : s->active) R = std::min(R, next_event(*r) - r->done);
-        R = std::max(R, 1);
-        const auto t0 = Clock::now();
-        ses_status st = ses_batch_step(s->batch, R, 1);
-        if (st == SES_OK) st = ses_batch_sync(s->batch, 600000);
-        const double round_ms = ms_since(t0);
-        if (st != SES_OK) {
-            const std::string err = ses_last_error();
-            for (const auto& r : s->active) retire(s, r, SES_REQ_FAILED, err);
-            s->active.clear();
-            continue;
-        }
-        double pts = 0;
-        for (const auto& r : s->active) pts += (double)grid_points(r->grid) * R;
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            ++s->rounds;
-            s->gridpt_steps += pts;
-            s->busy_ms += round_ms;
-        }
-        // observations of this round: every member at an observation point or done, one wait
-        std::vector<ses_handle> oh;
-        std::vector<double> olo, ohi;
-        std::vector<size_t> oi;
-        for (size_t i = 0; i < s->active.size(); ++i) {
-            Request& r = *s->active[i];
-            r.done += R;
-            if (r.done >= r.nsteps || (r.every > 0 && r.done % r.every == 0)) {
-                oh.push_back(r.h);
-                olo.push_back(r.xlo);
-                ohi.push_back(r.xhi);
-                oi.push_back(i);
+        // 4. new members join, then the next round is queued: up to the earliest
+        //    observation point or completion of any member
+        for (const auto& r : pending) {
+            bool c;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                c = r->cancel;
             }
-        }
-        std::vector<ses_observables> obs(oh.size());
-        if (!oh.empty()) st = ses_batch_observe_some(s->batch, oh.data(), (int)oh.size(), olo.data(), ohi.data(), obs.data());
-        if (st != SES_OK) {
-            const std::string err = ses_last_error();
-            for (const auto& r : s->active) retire(s, r, SES_REQ_FAILED, err);
-            s->active.clear();
-            continue;
-        }
-        for (size_t q = 0; q < oi.size(); ++q) {
-            Request& r = *s->active[oi[q]];
-            push_record(s, r, obs[q], r.done >= r.nsteps);
-        }
-        for (size_t i = 0; i < s->active.size();) {
-            std::shared_ptr<Request> r = s->active[i];
-            const bool fin = r->done >= r->nsteps;
-            if (fin) {
-                std::vector<double> out((size_t)grid_points(r->grid) * 2);
-                st = ses_gpu_read_psi(r->h, out.data());
-                const std::string err = st == SES_OK ? "" : ses_last_error();
-                {
-                    std::lock_guard<std::mutex> lk(s->mu);
-                    r->result.swap(out);
-                    r->result_ready = st == SES_OK;
-                }
-                retire(s, r, st == SES_OK ? SES_REQ_DONE : SES_REQ_FAILED, err);
-                s->active.erase(s->active.begin() + (long)i);
+            if (c) {
+                retire(s, r, SES_REQ_CANCELLED, "");
                 continue;
             }
-            ++i;
+            const ses_status st = ses_batch_add(s->batch, r->h);
+            if (st != SES_OK) {
+                retire(s, r, SES_REQ_FAILED, ses_last_error());
+                continue;
+            }
+            s->active.push_back(r);
+        }
+        pending.clear();
+        if (!s->active.empty()) {
+            R = s->max_round;
+            for (const auto& r : s->active) R = std::min(R, next_event(*r) - r->done);
+            R = std::max(R, 1);
+            t_round = Clock::now();
+            const ses_status st = ses_batch_step(s->batch, R, 1);
+            if (st != SES_OK)
+                fail_active(ses_last_error());
+            else
+                inflight = true;
+        }
+
+        // 5. results of the requests that finished, read back while the round runs
+        for (const auto& r : finishing) {
+            std::vector<double> out((size_t)grid_points(r->grid) * 2);
+            const ses_status st = ses_gpu_read_psi(r->h, out.data());
+            const std::string err = st == SES_OK ? "" : ses_last_error();
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                r->result.swap(out);
+                r->result_ready = st == SES_OK;
+            }
+            // with a round in flight the handle is freed after it (its bytes stay counted until then)
+            if (inflight) {
+                publish(s, r, st == SES_OK ? SES_REQ_DONE : SES_REQ_FAILED, err);
+                zombies.push_back(r);
+            } else {
+                retire(s, r, st == SES_OK ? SES_REQ_DONE : SES_REQ_FAILED, err);
+            }
+        }
+        finishing.clear();
+        if (!inflight && s->active.empty() && pending.empty()) {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (s->queue.empty()) s->idle.notify_all();
         }
     }
+    for (const auto& r : zombies) release_handle(s, r);
     std::lock_guard<std::mutex> lk(s->mu);
     s->idle.notify_all();
 }
