@@ -1,5 +1,5 @@
 // Device building blocks of the split-operator step: complex arithmetic,
-// in-register radix-2/3/4/5/6/8/10/16/20 DFTs, and one Stockham autosort stage over a
+// in-register radix-2/3/4/5/6/8/10/12/16/20 DFTs, and one Stockham autosort stage over a
 // tile of L lines held in shared memory.
 //
 // The line FFT is the forward unnormalised transform X_k = sum_n x_n e^{-2 pi i kn/N}
@@ -298,6 +298,28 @@ __device__ __forceinline__ void dft10(cx<T>* v) {
     v[9] = a[4] - b[4];
 }
 
+// 12 = 4 x 3 by the same mapping: input n = (3 n1 + 4 n2) mod 12, output
+// k = (9 k1 + 4 k2) mod 12 (3^{-1} = 3 mod 4, 4^{-1} = 1 mod 3).
+template <typename T>
+__device__ __forceinline__ void dft12(cx<T>* v) {
+    cx<T> a[4][3];
+#pragma unroll
+    for (int n2 = 0; n2 < 3; ++n2) {
+        cx<T> c[4];
+#pragma unroll
+        for (int n1 = 0; n1 < 4; ++n1) c[n1] = v[(3 * n1 + 4 * n2) % 12];
+        dft4(c);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) a[k1][n2] = c[k1];
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        dft3(a[k1]);
+#pragma unroll
+        for (int k2 = 0; k2 < 3; ++k2) v[(9 * k1 + 4 * k2) % 12] = a[k1][k2];
+    }
+}
+
 // 20 = 4 x 5 by the same mapping: input n = (5 n1 + 4 n2) mod 20, output
 // k = (5 k1 + 16 k2) mod 20 (5^{-1} = 1 mod 4, 4^{-1} = 4 mod 5).
 template <typename T>
@@ -329,6 +351,7 @@ __device__ __forceinline__ void dft(cx<T>* v) {
     else if constexpr (R == 6) dft6(v);
     else if constexpr (R == 8) dft8(v);
     else if constexpr (R == 10) dft10(v);
+    else if constexpr (R == 12) dft12(v);
     else if constexpr (R == 16) dft16(v);
     else if constexpr (R == 20) dft20(v);
 }

@@ -264,15 +264,22 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
         const bool wantm = (MODE == XM_MID ? a.m_mid : a.m_store) && !mfull && mx;
         if (vt && (want || wantm)) {  // this warp's rows, 16-byte chunks spread over the lanes
             __syncwarp();  // the previous tile's reads of these rows are done
-            if (want) {
+            if (want) {  // line by line, lane-strided 16-byte chunks: constant offsets per copy
                 constexpr int CH = N * (int)sizeof(cx<T>) / 16;
                 const long long m0 = (blk * NW + warp) * LPW;
-                const cx<T>* tab = reinterpret_cast<const cx<T>*>(a.tb.vtab);
-                for (int c = lane; c < LPW * CH; c += 32) {
-                    const int ln = c / CH, ch = c - ln * CH;
-                    if (m0 + ln < a.nlines)
-                        cp_async16(reinterpret_cast<char*>(vt + (size_t)(warp * LPW + ln) * RP) + 16 * ch,
-                                   reinterpret_cast<const char*>(tab + (m0 + ln) * N) + 16 * ch);
+                const char* tsrc = reinterpret_cast<const char*>(reinterpret_cast<const cx<T>*>(a.tb.vtab) + m0 * N);
+                char* tdst = reinterpret_cast<char*>(vt + (size_t)warp * LPW * RP);
+#pragma unroll
+                for (int ln = 0; ln < LPW; ++ln) {
+                    if (m0 + ln < a.nlines) {
+#pragma unroll
+                        for (int k = 0; k < (CH + 31) / 32; ++k) {
+                            const int ch = lane + 32 * k;
+                            if (CH % 32 == 0 || ch < CH)
+                                cp_async16(tdst + ((size_t)ln * RP * sizeof(cx<T>) + 16 * ch),
+                                           tsrc + ((size_t)ln * N * sizeof(cx<T>) + 16 * ch));
+                        }
+                    }
                 }
             }
             if (wantm) {
