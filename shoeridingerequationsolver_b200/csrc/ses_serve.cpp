@@ -293,8 +293,11 @@ void worker_main(ses_server_s* s) {
                     for (size_t i = 0; i < s->active.size();) {
                         std::shared_ptr<Request> r = s->active[i];
                         if (r->done >= r->nsteps) {
-                            ses_batch_remove(s->batch, r->h);  // its own stream from now on
-                            finishing.push_back(r);
+                            // leaves the batch: its own stream from now on
+                            if (ses_batch_remove(s->batch, r->h) == SES_OK)
+                                finishing.push_back(r);
+                            else
+                                retire(s, r, SES_REQ_FAILED, ses_last_error());
                             s->active.erase(s->active.begin() + (long)i);
                             continue;
                         }
