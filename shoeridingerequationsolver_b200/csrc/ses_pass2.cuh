@@ -190,9 +190,9 @@ struct XShape {
     static constexpr int PITCH = XPad<N, E>::PITCH;
     static constexpr int per_warp = LPW * PITCH * (int)sizeof(cx<T>);
     static constexpr int NW = (48 * 1024) / per_warp >= 4 ? 4 : ((48 * 1024) / per_warp < 1 ? 1 : (48 * 1024) / per_warp);
-    // CTAs per SM the register allocation is sized for: 40 elements per thread
-    // need more than the 128 registers of four 4-warp CTAs
-    static constexpr int MINB = E >= 40 ? 2 : 4;
+    // CTAs per SM the register allocation is sized for: 20 or more elements per
+    // thread need more than the 128 registers of four 4-warp CTAs
+    static constexpr int MINB = E >= 40 ? 2 : (E >= 20 ? 3 : 4);
     // Pitch of the staged potential-table rows of the batched pass: a
     // half-warp reads 16/TL lines at the same positions, each line covering 2 TL
     // banks with 64-bit elements; a pitch of TL mod 16 puts those lines on
