@@ -160,6 +160,16 @@ def test_batch_run_equals_separate_calls(ses, prec):
         run_ops.append(a)
         sep_ops.append(b)
         inputs.append(None if i == 2 else np.ascontiguousarray(psi))
+    # a 65536-point line: long lines step member by member on the batch stream
+    g1 = ses.line_grid(ses.Grid1D(-200.0, 200.0, 65536))
+    V1 = scenes.harmonic(g1, 0.05)
+    p1 = scenes.gaussian(g1, (3.0, 0.0, 0.0), (1.0, 1.0, 1.0), (0.5, 0.0, 0.0))
+    for ops in (run_ops, sep_ops):
+        op = ses.SplitOperator3D(g1, V1, 0.005, precision=prec, psi0=p1)
+        op.set_absorber_separable(scenes.mask_profiles(g1, 0.1)[0], np.ones(1), np.ones(1))
+        ops.append(op)
+    shapes.append((65536, 1, 1))
+    inputs.append(np.ascontiguousarray(p1 * np.exp(0.3j)))
     outputs = [None if i == 3 else np.full(op.grid.size(), np.nan, complex) for i, op in enumerate(run_ops)]
     with ses.Batch(run_ops) as br, ses.Batch(sep_ops) as bs:
         obs_run = br.run(7, psi_in=inputs, psi_out=outputs, absorb=True, xlo=0.0, xhi=math.inf)
