@@ -111,6 +111,7 @@ public:
     }
 
     double dt() const noexcept { return dt_; }
+    const Grid3D& grid() const noexcept { return grid_; }
 
     std::vector<cd> half_potential_phase() const {
         std::vector<cd> t(static_cast<std::size_t>(grid_.size()));
@@ -173,6 +174,68 @@ public:
 private:
     SplitOperator3D op_;
     int n_;
+};
+
+// Many propagations advanced together (no counterpart in the reference core,
+// whose directors loop over instances on the CPU: core/src/parallel.ixx:195-238).
+// Members stay owned by the caller and must outlive their membership.
+class Batch {
+public:
+    Batch() { check(ses_batch_create(&b_)); }
+    Batch(const Batch&) = delete;
+    Batch& operator=(const Batch&) = delete;
+    ~Batch() {
+        if (b_) ses_batch_destroy(b_);
+    }
+
+    void add(SplitOperator3D& op) {
+        check(ses_batch_add(b_, op.handle()));
+        members_.push_back(&op);
+    }
+    void remove(SplitOperator3D& op) {
+        check(ses_batch_remove(b_, op.handle()));
+        for (std::size_t i = 0; i < members_.size(); ++i)
+            if (members_[i] == &op) {
+                members_.erase(members_.begin() + static_cast<std::ptrdiff_t>(i));
+                break;
+            }
+    }
+    std::size_t size() const noexcept { return members_.size(); }
+    void step(int nsteps, bool absorb = false) { check(ses_batch_step(b_, nsteps, absorb ? 1 : 0)); }
+    std::vector<ses_observables> observe(double xlo = -1e300, double xhi = 1e300) {
+        std::vector<ses_observables> out(members_.size());
+        check(ses_batch_observe(b_, xlo, xhi, out.data(), static_cast<int>(out.size())));
+        return out;
+    }
+    void sync(int timeout_ms = 0) { check(ses_batch_sync(b_, timeout_ms)); }
+
+    // One host round trip of every member (ses_batch_run): upload in[i] (skipped
+    // where null), nsteps steps, observables, read back into out[i] (skipped
+    // where null).  Fields match the members in the order they were added.
+    std::vector<ses_observables> run(const std::vector<Field3D*>& in, int nsteps, bool absorb,
+                                     const std::vector<Field3D*>& out, double xlo = -1e300,
+                                     double xhi = 1e300) {
+        const std::size_t m = members_.size();
+        if ((!in.empty() && in.size() != m) || (!out.empty() && out.size() != m))
+            throw std::invalid_argument("one field (or null) per member");
+        std::vector<const double*> pin(m, nullptr);
+        std::vector<double*> pout(m, nullptr);
+        for (std::size_t i = 0; i < m; ++i) {
+            for (Field3D* f : {in.empty() ? nullptr : in[i], out.empty() ? nullptr : out[i]})
+                if (f && f->size() != members_[i]->grid().size())
+                    throw std::invalid_argument("field does not match its member's grid");
+            if (!in.empty() && in[i]) pin[i] = raw(in[i]->data());
+            if (!out.empty() && out[i]) pout[i] = raw(out[i]->data());
+        }
+        std::vector<ses_observables> obs(m);
+        check(ses_batch_run(b_, in.empty() ? nullptr : pin.data(), nsteps, absorb ? 1 : 0, xlo, xhi,
+                            obs.data(), out.empty() ? nullptr : pout.data(), static_cast<int>(m), 0));
+        return obs;
+    }
+
+private:
+    ses_batch b_ = nullptr;
+    std::vector<SplitOperator3D*> members_;
 };
 
 }  // namespace ses::gpu

@@ -112,6 +112,51 @@ int main() {
         const double nrm = seso_norm1d(-40, 40, 1024, reinterpret_cast<const double*>(psi.data()));
         EXPECT(std::fabs(nrm - 1.0) < 1e-12, "1D free packet conserves norm");
     }
+    {  // a director sweeping several scenes through one batch: 16^3 and 32^3 (batched
+       // kernels) and 8^3 (member by member), complex64, one host round trip each
+        const int sizes[3] = {16, 32, 8};
+        std::vector<ses::gpu::SplitOperator3D> ops;
+        std::vector<ses::gpu::Field3D> in, out;
+        std::vector<std::vector<cd>> want;
+        for (int s : sizes) {
+            const double box[6] = {-4, 4, -4, 4, -4, 4};
+            const int n[3] = {s, s, s};
+            const double c[3] = {0, 0, 0}, r0[3] = {0.5, 0, 0}, sg[3] = {1.0, 1.0, 1.0}, k0[3] = {1, 0, 0};
+            const int N = s * s * s;
+            std::vector<double> V(N);
+            seso_harmonic3d(box, n, 1.0, c, V.data());
+            const ses::gpu::Grid3D g{{-4, 4, s}, {-4, 4, s}, {-4, 4, s}};
+            ops.emplace_back(g, V, 0.01, 1.0, SES_C64);
+            in.emplace_back(g);
+            out.emplace_back(g);
+            seso_gaussian3d(box, n, r0, sg, k0, reinterpret_cast<double*>(in.back().data().data()));
+            std::vector<cd> ref = in.back().data();
+            seso_step3d(box, n, V.data(), 0.01, 1.0, nullptr, reinterpret_cast<double*>(ref.data()), 15);
+            want.push_back(ref);
+        }
+        ses::gpu::Batch b;
+        for (auto& op : ops) b.add(op);
+        const std::vector<ses_observables> obs = b.run({&in[0], &in[1], &in[2]}, 15, false, {&out[0], &out[1], &out[2]});
+        double worst = 0;
+        for (std::size_t m = 0; m < ops.size(); ++m) {
+            double num = 0, den = 0;
+            for (std::size_t i = 0; i < want[m].size(); ++i) {
+                num += std::norm(out[m].data()[i] - want[m][i]);
+                den += std::norm(want[m][i]);
+            }
+            worst = std::fmax(worst, std::sqrt(num / den));
+        }
+        std::printf("  batch round trip: worst rel L2 vs the FP64 core %.3e\n", worst);
+        EXPECT(worst < 1e-5, "batch round trip vs FP64 core");
+        EXPECT(obs.size() == 3 && std::fabs(obs[1].norm - 1.0) < 1e-5, "batch observables");
+        bool threw = false;
+        try {
+            b.run({&in[1], &in[0], &in[2]}, 1, false, {});
+        } catch (const std::invalid_argument&) {
+            threw = true;
+        }
+        EXPECT(threw, "batch run rejects a field of the wrong size");
+    }
     std::printf("%s (%d failures)\n", failures ? "FAILED" : "OK", failures);
     return failures ? 1 : 0;
 }
