@@ -260,6 +260,7 @@ struct ses_solver {
     unsigned* herr = nullptr;  // pinned host copy
     int sms = 148;
     bool pipelined = true;
+    bool pdl = true;  // single-field passes launched with programmatic stream serialization
     int xsel = 0;                  // pipelined contiguous-pass variant (-1: register path)
     int ssel[3] = {0, 0, 0};       // pipelined strided-pass variant per axis (-1: register path)
     ses_batch_s* batch = nullptr;  // batch this handle belongs to (its stream is the batch's)
@@ -432,6 +433,25 @@ XKernel<T> skernel(int mode) {
     }
 }
 
+// Launch of a single-field pass kernel, with programmatic stream serialization
+// when the handle allows it (the kernel starts while the previous kernel of the
+// stream drains and waits in pdl_wait before touching any field).
+template <typename... KArgs, typename... Args>
+void launch_pass(bool pdl, void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                 Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
 template <typename T>
 ses_status launch(const ses_solver* h, int axis, int mode, const PassArgs<T>& a, cudaStream_t s) {
     const PassPlan& pp = h->pp[axis];
@@ -448,7 +468,7 @@ ses_status launch(const ses_solver* h, int axis, int mode, const PassArgs<T>& a,
             pa.ntiles = (int)((pp.nlines + v.lpc - 1) / v.lpc);
             pa.err = h->derr;
             const int grid = std::min(pa.ntiles, h->sms * v.bps[mode]);
-            v.k[mode]<<<grid, 32 * v.warps, v.smem[mode], s>>>(a, pa);
+            launch_pass(h->pdl, v.k[mode], (unsigned)grid, 32u * v.warps, v.smem[mode], s, a, pa);
             done = true;
         } else if (h->pipelined && axis != 0 && ss >= 0 && ss < (int)e->sv.size() && e->sv[ss].k[mode] &&
                    e->sv[ss].bps[mode] > 0) {
@@ -464,17 +484,18 @@ ses_status launch(const ses_solver* h, int axis, int mode, const PassArgs<T>& a,
                 pa.nbox = n / pa.rows_per_box;
                 pa.err = h->derr;
                 const int grid = std::min(pa.ntiles, h->sms * v.bps[mode]);
-                v.k[mode]<<<grid, v.ls * tl, v.smem, s>>>(a, h->tmap[buf][axis][ss], pa);
+                launch_pass(h->pdl, v.k[mode], (unsigned)grid, (unsigned)(v.ls * tl), v.smem, s, a,
+                            h->tmap[buf][axis][ss], pa);
                 done = true;
             }
         }
         if (!done) {
             PassKernel<T> k = axis == 0 ? e->xk[mode] : e->sk[mode];
-            k<<<pp.cgrid, pp.cblock, pp.csmem, s>>>(a);
+            launch_pass(h->pdl, k, pp.cgrid, pp.cblock, pp.csmem, s, a);
         }
     } else {
         XKernel<T> k = axis == 0 ? xkernel<T>(mode) : skernel<T>(mode);
-        k<<<pp.grid, pp.g.nthreads, pp.smem, s>>>(a);
+        launch_pass(h->pdl, k, pp.grid, (unsigned)pp.g.nthreads, pp.smem, s, a);
     }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
@@ -985,6 +1006,7 @@ void apply_selection(ses_solver* h) {
         else h->ssel[a] = it->second;
     }
     if (const char* e = std::getenv("SES_XVAR")) h->xsel = std::atoi(e);
+    if (const char* e = std::getenv("SES_PDL")) h->pdl = std::atoi(e) != 0;
     if (const char* e = std::getenv("SES_SVAR")) h->ssel[1] = h->ssel[2] = std::atoi(e);
 }
 

@@ -276,8 +276,15 @@ constexpr int kSModes = 7;
 // Contiguous-axis (x) pass.  Tile = L consecutive x-lines, loaded and stored
 // with coalesced accesses; shared layout [l][e] with an odd pitch.
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch: a single-field pass may be launched while the
+// previous kernel of its stream drains; it waits here, before touching any
+// field, until that kernel has completed and its writes are visible (a no-op
+// for a normal launch).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(512, 1) xpass_kernel(const PassArgs<T> a) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ Geo g;  // stage tables are indexed at run time: keep them out of parameter space
     if (threadIdx.x == 0) g = a.g;
@@ -395,6 +402,7 @@ __global__ void __launch_bounds__(512, 1) xpass_kernel(const PassArgs<T> a) {
 // ---------------------------------------------------------------------------
 template <typename T, int MODE>
 __global__ void __launch_bounds__(512, 1) spass_kernel(const PassArgs<T> a) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ Geo g;  // stage tables are indexed at run time: keep them out of parameter space
     if (threadIdx.x == 0) g = a.g;

@@ -391,6 +391,7 @@ template <typename T, int MODE, int N, int E, int R0, int R1, int R2>
 __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, XShape<T, N, E>::MINB) xpass2_kernel(const PassArgs<T> a) {
     using XS = XShape<T, N, E>;
     __shared__ cx<T> xb[XS::NW * XS::LPW * XS::PITCH];
+    pdl_wait();
     xpass2_body<T, MODE, N, E, R0, R1, R2>(a, (long long)blockIdx.x, xb, a.stw, a.stwl);
 }
 
@@ -551,6 +552,7 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L>
 __global__ void __launch_bounds__(L*(N / E), 1) spass2_kernel(const PassArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smraw[];
+    pdl_wait();
     spass2_body<T, MODE, N, E, R0, R1, R2, L>(a, (long long)blockIdx.x, reinterpret_cast<cx<T>*>(smraw), a.stw,
                                               a.stwl);
 }

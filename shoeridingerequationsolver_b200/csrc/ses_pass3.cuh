@@ -203,6 +203,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, int NBUF, int MINB>
 __global__ void __launch_bounds__(L*(N / E), MINB)
     spass3_kernel(const PassArgs<T> a, const __grid_constant__ CUtensorMap tmap, const PipeArgs pa) {
+    pdl_wait();
     spass3_body<T, MODE, N, E, R0, R1, R2, L, NBUF>(OneField<T>{a, &tmap}, pa);
 }
 
@@ -396,6 +397,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
 
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int NW, int NBUF, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T> a, const PipeArgs pa) {
+    pdl_wait();
     xpass3_body<T, MODE, N, E, R0, R1, R2, NW, NBUF>(OneField<T>{a, nullptr}, pa);
 }
 
