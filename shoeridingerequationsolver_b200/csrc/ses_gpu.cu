@@ -433,9 +433,9 @@ XKernel<T> skernel(int mode) {
     }
 }
 
-// Launch of a single-field pass kernel, with programmatic stream serialization
-// when the handle allows it (the kernel starts while the previous kernel of the
-// stream drains and waits in pdl_wait before touching any field).
+// Launch of a pass kernel (single-field or batched), with programmatic stream
+// serialization when the handle allows it (the kernel starts while the previous
+// kernel of the stream drains and waits in pdl_wait before touching any field).
 template <typename... KArgs, typename... Args>
 void launch_pass(bool pdl, void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
                  Args&&... args) {
@@ -1819,11 +1819,12 @@ ses_status class_launch(const ses_batch_s* b, const BatchClass& c, int prog, boo
         if (axis == 0) {
             const auto& v = e->xv[c.xvar];
             const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * v.bbps[mode]));
-            v.kb[mode]<<<grid, 32 * v.warps, v.smemb[mode], s>>>(args, w, pa);
+            launch_pass(h0->pdl, v.kb[mode], grid, 32u * v.warps, v.smemb[mode], s, args, w, pa);
         } else {
             const auto& v = e->sv[c.svar[q]];
             const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * v.bbps[mode]));
-            v.kb[mode]<<<grid, v.ls * (n / e->e), v.smem, s>>>(args, maps + (size_t)q * nm, w, pa);
+            launch_pass(h0->pdl, v.kb[mode], grid, (unsigned)(v.ls * (n / e->e)), v.smem, s, args,
+                        maps + (size_t)q * nm, w, pa);
         }
         const cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess)
@@ -1839,11 +1840,11 @@ ses_status class_launch(const ses_batch_s* b, const BatchClass& c, int prog, boo
     if (axis == 0) {
         const int bps = std::max(1, e->xb_bps[mode]);
         const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * bps));
-        e->xb[mode]<<<grid, pp.cblock, e->xbsm, s>>>(args, w);
+        launch_pass(h0->pdl, e->xb[mode], grid, pp.cblock, e->xbsm, s, args, w);
     } else {
         const int bps = std::max(1, e->sb_bps[mode]);
         const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * bps));
-        e->sb[mode]<<<grid, pp.cblock, pp.csmem + e->twb, s>>>(args, w);
+        launch_pass(h0->pdl, e->sb[mode], grid, pp.cblock, pp.csmem + e->twb, s, args, w);
     }
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return fail(SES_EDEVICE, std::string("batched pass launch: ") + cudaGetErrorString(err));

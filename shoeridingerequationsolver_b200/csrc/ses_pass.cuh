@@ -276,10 +276,10 @@ constexpr int kSModes = 7;
 // Contiguous-axis (x) pass.  Tile = L consecutive x-lines, loaded and stored
 // with coalesced accesses; shared layout [l][e] with an odd pitch.
 // ---------------------------------------------------------------------------
-// Programmatic dependent launch: a single-field pass may be launched while the
+// Programmatic dependent launch: a pass kernel may be launched while the
 // previous kernel of its stream drains; it waits here, before touching any
-// field, until that kernel has completed and its writes are visible (a no-op
-// for a normal launch).
+// field or argument table, until that kernel has completed and its writes are
+// visible (a no-op for a normal launch).
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 template <typename T, int MODE>

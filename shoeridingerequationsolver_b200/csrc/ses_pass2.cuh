@@ -578,6 +578,7 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, XShape<T, N, E>::MIN
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T>* tw = reinterpret_cast<cx<T>*>(smraw);
     cx<T>* vt = reinterpret_cast<cx<T>*>(smraw + TW::bytes);  // XBatchSmem: rows of the potential table
+    pdl_wait();
     if (blockIdx.x < w.total) TW::load(tw, args[0].stw, args[0].stwl);  // one plan per class
     __syncthreads();
     for (uint32_t t = blockIdx.x; t < w.total; t += gridDim.x) {
@@ -602,6 +603,7 @@ __global__ void __launch_bounds__(L*(N / E), 1)
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T>* tile = reinterpret_cast<cx<T>*>(smraw);
     cx<T>* tw = tile + (size_t)N * L;
+    pdl_wait();
     if (blockIdx.x < w.total) TW::load(tw, args[0].stw, args[0].stwl);
     __syncthreads();
     for (uint32_t t = blockIdx.x; t < w.total; t += gridDim.x) {

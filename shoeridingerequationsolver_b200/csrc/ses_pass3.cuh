@@ -212,6 +212,7 @@ template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, int
 __global__ void __launch_bounds__(L*(N / E), MINB)
     sbatch3_kernel(const PassArgs<T>* __restrict__ args, const CUtensorMap* maps, const BatchWork w,
                    const PipeArgs pa) {
+    pdl_wait();
     spass3_body<T, MODE, N, E, R0, R1, R2, L, NBUF>(ManyFields<T>{args, maps, w}, pa);
 }
 
@@ -404,6 +405,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) xpass3_kernel(const PassArgs<T>
 template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int NW, int NBUF, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB)
     xbatch3_kernel(const PassArgs<T>* __restrict__ args, const BatchWork w, const PipeArgs pa) {
+    pdl_wait();
     xpass3_body<T, MODE, N, E, R0, R1, R2, NW, NBUF>(ManyFields<T>{args, nullptr, w}, pa);
 }
 
