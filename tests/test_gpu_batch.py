@@ -194,3 +194,29 @@ def test_batch_run_equals_separate_calls(ses, prec):
             br.run(1, psi_in=inputs[:2])
     for op in run_ops + sep_ops:
         op.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+def test_programmatic_launch_changes_no_bits(ses, prec, monkeypatch):
+    """Passes launched with programmatic dependent launch (the default) wait for the
+    previous kernel before touching any field, so the results equal those of plain
+    launches bit for bit -- single handles and batches."""
+    box = (8.0, 7.0, 6.0)
+    shapes = [(64, 64, 64), (48, 48, 48), (96, 96, 1), (16, 16, 16)]
+    runs = {}
+    for pdl in ("0", "1"):
+        monkeypatch.setenv("SES_PDL", pdl)   # read when a handle is created
+        single = [make_member(ses, s, box, prec, seed=500 + i)[0] for i, s in enumerate(shapes)]
+        batched = [make_member(ses, s, box, prec, seed=500 + i)[0] for i, s in enumerate(shapes)]
+        for op in single:
+            op.advance(13, absorb=True)
+        with ses.Batch(batched) as b:
+            b.step(13, absorb=True)
+            b.sync()
+            runs[pdl] = ([op.readback() for op in single], [op.readback() for op in batched])
+        for op in single + batched:
+            op.close()
+    for kind in (0, 1):
+        for a, b, s in zip(runs["0"][kind], runs["1"][kind], shapes):
+            assert np.array_equal(a, b), (kind, s)
