@@ -136,3 +136,28 @@ def test_serve_cancel_and_continue(ses):
             srv.result(rid)
         psi, lat = srv.result(sid)
         assert np.all(np.isfinite(psi)) and lat > 0
+
+
+@pytest.mark.gpu
+def test_serve_mixed_precision_and_mass(ses):
+    """A complex128 request with an effective mass, served next to complex64 ones
+    that start and finish while it runs, ends where the same handle stepped alone
+    ends (batched kernels vs single-field kernels: rounding-level agreement)."""
+    heavy = spec(ses, (48, 48, 48), 8.0, 31, nsteps=240, every=60)
+    heavy.update(precision="c128", mass=0.38)
+    light = [spec(ses, (32, 32, 32), 7.0, 40 + i, nsteps=20 + 15 * i, every=0) for i in range(6)]
+    with ses.Server(budget_bytes=8 * 2**30, max_round_steps=40) as srv:
+        hid = srv.submit(**heavy)
+        lids = [srv.submit(**s) for s in light]
+        srv.wait_idle(300000)
+        for rid in [hid] + lids:
+            assert srv.poll(rid)[0] == "done"
+        psi, _ = srv.result(hid)
+        st = srv.stats()
+        assert st["completed"] == 7 and st["failed"] == 0 and st["bytes_in_use"] == 0
+    op = ses.SplitOperator3D(heavy["grid"], heavy["V"], heavy["dt"], 0.38, precision="c128", psi0=heavy["psi0"])
+    op.set_absorber_separable(*heavy["mask"])
+    op.advance(240, absorb=True)
+    want = op.readback()
+    op.close()
+    assert rel(psi, want) <= 1e-13
