@@ -36,6 +36,9 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Requests admitted (handles created) per round while other requests run.
+constexpr int kAdmitPerRound = 4;
+
 ses_status sfail(ses_status s, const std::string& msg) {
     sesk::set_last_error(msg);
     return s;
@@ -222,7 +225,11 @@ void worker_main(ses_server_s* s) {
                 finishing.empty())
                 break;
             size_t room = s->budget > s->used ? s->budget - s->used : 0;
-            while (!s->queue.empty()) {
+            // while the device has work, admit a few requests per round (their set-up
+            // overlaps the round); with nothing to run, admit one and start stepping it
+            const bool busy = inflight || !s->active.empty() || !pending.empty();
+            const size_t cap = busy ? (size_t)kAdmitPerRound : 1;
+            while (!s->queue.empty() && take.size() < cap) {
                 std::shared_ptr<Request> r = s->queue.front();
                 if (r->cancel) {
                     r->state = SES_REQ_CANCELLED;
