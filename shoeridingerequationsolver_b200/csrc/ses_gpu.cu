@@ -437,8 +437,8 @@ XKernel<T> skernel(int mode) {
 // serialization when the handle allows it (the kernel starts while the previous
 // kernel of the stream drains and waits in pdl_wait before touching any field).
 template <typename... KArgs, typename... Args>
-void launch_pass(bool pdl, void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
-                 Args&&... args) {
+cudaError_t launch_pass(bool pdl, void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem,
+                        cudaStream_t s, Args&&... args) {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
@@ -449,7 +449,7 @@ void launch_pass(bool pdl, void (*k)(KArgs...), unsigned grid, unsigned block, s
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = pdl ? 1 : 0;
-    cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+    return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);  // also recorded for cudaGetLastError
 }
 
 template <typename T>
