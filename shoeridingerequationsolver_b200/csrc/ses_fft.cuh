@@ -55,10 +55,6 @@ template <typename T>
 __device__ __forceinline__ cx<T> operator*(cx<T> a, cx<T> b) {
     return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-template <typename T>
-__device__ __forceinline__ cx<T> scale(cx<T> a, T s) {
-    return mk<T>(a.x * s, a.y * s);
-}
 // a * s for an FP64 scale s such as 1/N, which is not a power of two for
 // radix-3/5 sizes: complex64 carries s as hi + lo, so that the scale applied
 // every step has no systematic rounding (a plain FP32 1/N is off by up to 6e-8,
@@ -134,14 +130,8 @@ __device__ __forceinline__ CK<T> ck(double c) {
     }
 }
 
-template <typename T>
-__device__ __forceinline__ T kmul(T a, CK<T> c) {
-    if constexpr (sizeof(T) == 4) return fmaf(a, c.hi, a * c.lo);
-    else return a * c.hi;
-}
-
-// a * c for complex a and a real compensated constant (componentwise kmul;
-// complex64 as two packed FP32 operations).
+// a * c for complex a and a real compensated constant c = c.hi + c.lo,
+// componentwise fma(a, c.hi, a * c.lo) (complex64 as two packed FP32 operations).
 template <typename T>
 __device__ __forceinline__ cx<T> kmulc(cx<T> a, CK<T> c) {
     if constexpr (sizeof(T) == 4)

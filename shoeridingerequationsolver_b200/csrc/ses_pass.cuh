@@ -165,10 +165,6 @@ __device__ __forceinline__ cx<T> apply_diag_tv(cx<T> v, int kind, cx<T> tab, int
     }
 }
 
-__device__ __forceinline__ double mask_at(const Tables& tb, long long f, int i, int j, int k) {
-    return tb.maskfull ? tb.maskfull[f] : tb.mask1[0][i] * tb.mask1[1][j] * tb.mask1[2][k];
-}
-
 // psi_k * K / N then conj (inverse FFT start); complex64: FP32 on the delta form.
 __device__ __forceinline__ cx<float> kinetic_conj_f(cx<float> v, cx<float> d, double kscale) {
     return cconj(scale_d(add_mul(v, d), kscale));

@@ -44,14 +44,9 @@ __device__ __forceinline__ cx<T> tw4_mul(cx<T> v, const Tables& tb, long long f)
     return twmul(v, reinterpret_cast<const cx<T>*>(tb.tw4), reinterpret_cast<const cx<T>*>(tb.tw4l), (int)f);
 }
 
-// Offset of stage p's table: tables are R_p x Ns_p entries, w^{r k N/(Ns R)} at [r*Ns + k].
-template <int R0, int R1, int R2>
-struct StageOff {
-    static constexpr int o0 = 0;
-    static constexpr int o1 = R0 * 1;
-    static constexpr int o2 = o1 + R1 * R0;
-};
-
+// One Stockham stage of radix R after NS points per butterfly group: twiddle
+// then DFT of each of the thread's E/R butterflies.  A stage's table holds
+// R x NS entries, w^{r k N/(NS R)} at [OFF + r*NS + k].
 template <typename T, int N, int E, int TL, int R, int NS, int OFF>
 __device__ __forceinline__ void rstage(cx<T> (&v)[E], int q, const cx<T>* __restrict__ twh,
                                        const cx<T>* __restrict__ twl) {
