@@ -1,5 +1,5 @@
 // Device building blocks of the split-operator step: complex arithmetic,
-// in-register radix-2/3/4/5/6/8/10/12/16/20 DFTs, and one Stockham autosort stage over a
+// in-register radix-2/3/4/5/6/8/10/12/16/20/32 DFTs, and one Stockham autosort stage over a
 // tile of L lines held in shared memory.
 //
 // The line FFT is the forward unnormalised transform X_k = sum_n x_n e^{-2 pi i kn/N}
@@ -218,6 +218,47 @@ __device__ __forceinline__ void dft16(cx<T>* v) {
     }
 }
 
+// 32 = 2 x 16: the even and odd samples' 16-point DFTs, the odd ones rotated by
+// w32^k = cos(pi k/16) - i sin(pi k/16), then one radix-2 combination.
+template <typename T>
+__device__ __forceinline__ void dft32(cx<T>* v) {
+    const CK<T> c1 = ck<T>(0.98078528040323044913);  // cos(pi/16)
+    const CK<T> s1 = ck<T>(0.19509032201612826785);  // sin(pi/16)
+    const CK<T> c2 = ck<T>(0.92387953251128675613);  // cos(pi/8)
+    const CK<T> s2 = ck<T>(0.38268343236508977173);  // sin(pi/8)
+    const CK<T> c3 = ck<T>(0.83146961230254523708);  // cos(3pi/16)
+    const CK<T> s3 = ck<T>(0.55557023301960222474);  // sin(3pi/16)
+    const CK<T> h = ck<T>(0.70710678118654752440);   // cos(pi/4)
+    cx<T> e[16], o[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        e[k] = v[2 * k];
+        o[k] = v[2 * k + 1];
+    }
+    dft16(e);
+    dft16(o);
+    o[1] = rotc(o[1], c1, s1);
+    o[2] = rotc(o[2], c2, s2);
+    o[3] = rotc(o[3], c3, s3);
+    o[4] = rotc(o[4], h, h);
+    o[5] = rotc(o[5], s3, c3);
+    o[6] = rotc(o[6], s2, c2);
+    o[7] = rotc(o[7], s1, c1);
+    o[8] = mul_mi(o[8]);
+    o[9] = rotc(o[9], neg(s1), c1);
+    o[10] = rotc(o[10], neg(s2), c2);
+    o[11] = rotc(o[11], neg(s3), c3);
+    o[12] = rotc(o[12], neg(h), h);
+    o[13] = rotc(o[13], neg(c3), s3);
+    o[14] = rotc(o[14], neg(c2), s2);
+    o[15] = rotc(o[15], neg(c1), s1);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        v[k] = e[k] + o[k];
+        v[k + 16] = e[k] - o[k];
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void dft3(cx<T>* v) {
     const CK<T> hs3 = ck<T>(0.86602540378443864676);  // sin(2 pi/3)
@@ -344,6 +385,7 @@ __device__ __forceinline__ void dft(cx<T>* v) {
     else if constexpr (R == 12) dft12(v);
     else if constexpr (R == 16) dft16(v);
     else if constexpr (R == 20) dft20(v);
+    else if constexpr (R == 32) dft32(v);
 }
 
 // ---------------------------------------------------------------------------
