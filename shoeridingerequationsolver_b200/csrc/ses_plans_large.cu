@@ -1,5 +1,5 @@
 // Compiled plans: 512 = 8 x 8 x 8 (complex64 strided passes: 16 x 32), 1024 = 16 x 8 x 8
-// (complex64 only).
+// (complex64 strided passes: 32 x 32; complex64 only).
 #include "ses_plans.cuh"
 
 namespace sesk {
@@ -18,5 +18,10 @@ void register_plans_large(std::vector<PlanEntry<float>>& f, std::vector<PlanEntr
     add_x_variant<double, 512, 16, 8, 8, 8, 2, 2, 1>(d.back());
     add_s_variant<double, 512, 16, 8, 8, 8, 8, 2, 1>(d.back());
     f.push_back(make_plan_entry<float, 1024, 32, 16, 8, 8, 8>());
+    f.back().kinds = 1;
+    // complex64 1024 strided passes (the y pass of 1024^2 planes): 32x32, two stages
+    f.push_back(make_plan_entry<float, 1024, 32, 32, 32, 1, 4>());
+    f.back().kinds = 2;
+    add_s_variant<float, 1024, 32, 32, 32, 1, 4, 2, 2>(f.back());
 }
 }  // namespace sesk

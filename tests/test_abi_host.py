@@ -206,7 +206,8 @@ COMPILED_PLANS = [(16, 16, (16,)), (32, 8, (8, 4)), (48, 12, (4, 4, 3)), (48, 12
                   (96, 24, (12, 8)),
                   (96, 12, (6, 4, 4)), (128, 16, (16, 8)), (160, 20, (10, 4, 4)), (160, 40, (20, 8)),
                   (256, 16, (16, 16)),
-                  (512, 16, (8, 8, 8)), (512, 32, (16, 32)), (1024, 32, (16, 8, 8))]
+                  (512, 16, (8, 8, 8)), (512, 32, (16, 32)), (1024, 32, (16, 8, 8)),
+                  (1024, 32, (32, 32))]
 
 
 def xpad(N, E):

@@ -163,6 +163,9 @@ STEP_CASES = [
      1.0),
     ("line_1024_free", ((-40, 40, 0, 1, 0, 1), (1024, 1, 1)), lambda o, b, n: np.zeros(1024),
      0.05, ((-15, 0, 0), (1, 1, 1), (2, 0, 0)), 30, 1.0),
+    # the serving mix's large planes: 1024-point rows and 1024-point strided columns
+    ("planar_1024sq_harmonic", ((-30, 30, -30, 30, 0, 1), (1024, 1024, 1)),
+     lambda o, b, n: o.harmonic3d(b, n, 0.5), 0.005, ((2, -1, 0), (1.5, 1.5, 1.0), (2, 0, 0)), 4, 1.0),
 ]
 
 
