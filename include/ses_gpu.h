@@ -200,6 +200,33 @@ SES_API ses_status ses_gpu_autotune(ses_handle h, int flags);
 SES_API ses_status ses_gpu_plan_info(ses_handle h, char* buf, size_t len);
 /* Device bytes held by the handle. */
 SES_API ses_status ses_gpu_footprint(ses_handle h, size_t* bytes);
+/* Failure-detection hook, the counterpart of the reference's 10 s fence timeout
+ * that marks the engine device_lost (solver/src/vk_compute.ixx:297-327): every
+ * wait inside this handle's pipelined (TMA-fed) passes is bounded by
+ * wait_cycles SM clock cycles (0: about 2 s, the default), and with
+ * extra_tx_bytes > 0 every tile's barrier expects that many bytes more than its
+ * copies deliver, so its wait runs out -- the pass then records the error,
+ * drains its copies (bounded) and returns, no load or store is changed, and the
+ * next ses_gpu_sync reports SES_ETIMEDOUT with the context still usable.  For
+ * tests of that path; (0, 0) restores normal operation.  Waits for queued work
+ * first; extra_tx_bytes <= 4096. */
+SES_API ses_status ses_gpu_set_wait_limit(ses_handle h, int64_t wait_cycles, uint32_t extra_tx_bytes);
+/* Engine::norm_and_peak (solver/src/vk_engine.ixx:1665-1692, shader
+ * solver/shaders/norm_peak.comp.slang): norm = sum |psi|^2 dV and peak =
+ * max |psi|^2 of the resident psi, FP64 sums folded in a fixed order
+ * (deterministic).  Either output may be NULL.  Blocks. */
+SES_API ses_status ses_gpu_norm_and_peak(ses_handle h, double* norm, double* peak);
+/* Engine::scale(s) (solver/src/vk_engine.ixx:2120-2133, shader
+ * solver/shaders/scale.comp.slang:12-19): psi <- factor * psi, the directors'
+ * drift renormalisation (scenario/src/base_director.ixx:340-352).  Queued on
+ * the handle's stream. */
+SES_API ses_status ses_gpu_scale(ses_handle h, double factor);
+/* Records the handle's step graph ahead of the first long step batch (the
+ * reference engine records its command buffers in Engine::initialize,
+ * solver/src/vk_engine.ixx:173-580), so that no capture happens inside a
+ * caller's timed or latency-critical region.  absorb selects the graph with or
+ * without the mask; psi is not touched. */
+SES_API ses_status ses_gpu_prepare(ses_handle h, int absorb);
 
 /* ---- allocation-free entry point ----
  * No counterpart in the reference.  For callers that cannot allocate device
@@ -250,6 +277,8 @@ SES_API ses_status ses_batch_remove(ses_batch b, ses_handle h);
  * first call after a membership change waits for queued work and uploads the
  * per-member pass arguments. */
 SES_API ses_status ses_batch_step(ses_batch b, int nsteps, int absorb);
+/* ses_gpu_prepare for every class of the batch (its per-class step graph). */
+SES_API ses_status ses_batch_prepare(ses_batch b, int absorb);
 /* ses_gpu_observe of every member, in the order they were added (count must be
  * the member count), with one wait for the whole batch. */
 SES_API ses_status ses_batch_observe(ses_batch b, double xlo, double xhi, ses_observables* out, int count);

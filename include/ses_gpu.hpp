@@ -8,8 +8,10 @@
 // device errors and expired bounded waits throw std::runtime_error.
 #pragma once
 
+#include <cmath>
 #include <complex>
 #include <cstddef>
+#include <memory>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -151,10 +153,176 @@ public:
     void sync(int timeout_ms = 0) const { check(ses_gpu_sync(h_, timeout_ms)); }
     ses_handle handle() const noexcept { return h_; }
 
+    // Engine::norm_and_peak / Engine::scale (solver/src/vk_engine.ixx:1665-1692, 2120-2133)
+    struct NormPeak {
+        double sum = 0.0;   // sum |psi|^2 dV
+        double peak = 0.0;  // max |psi|^2
+    };
+    NormPeak norm_and_peak() const {
+        NormPeak np;
+        check(ses_gpu_norm_and_peak(h_, &np.sum, &np.peak));
+        return np;
+    }
+    void scale(double s) { check(ses_gpu_scale(h_, s)); }
+    // records the step graph now rather than inside the first long advance
+    void prepare(bool absorb = false) { check(ses_gpu_prepare(h_, absorb ? 1 : 0)); }
+
 private:
     Grid3D grid_;
     double dt_;
     ses_handle h_ = nullptr;
+};
+
+// ImaginaryTimePropagator3D (core/src/imaginary_time.ixx:64-108): relax(psi, n)
+// renormalises after every step, as the reference.
+class ImaginaryTimePropagator3D {
+public:
+    ImaginaryTimePropagator3D(const Grid3D& g, const std::vector<double>& potential, double dtau,
+                              double mass = 1.0, ses_precision prec = SES_C128)
+        : grid_(g) {
+        if (static_cast<int>(potential.size()) != g.size())
+            throw std::invalid_argument("potential size does not match the grid");
+        const ses_grid_desc d = g.desc();
+        check(ses_gpu_create_imag(&d, prec, dtau, mass, potential.data(), nullptr, &h_));
+    }
+    ImaginaryTimePropagator3D(const ImaginaryTimePropagator3D&) = delete;
+    ImaginaryTimePropagator3D& operator=(const ImaginaryTimePropagator3D&) = delete;
+    ~ImaginaryTimePropagator3D() {
+        if (h_) ses_gpu_destroy(h_);
+    }
+    void relax(Field3D& psi, int nsteps) const {
+        if (psi.size() != grid_.size()) throw std::invalid_argument("field does not match the grid");
+        check(ses_gpu_write_psi(h_, raw(psi.data())));
+        check(ses_gpu_relax(h_, nsteps, 1, nullptr));
+        check(ses_gpu_read_psi(h_, raw(psi.data())));
+    }
+
+private:
+    Grid3D grid_;
+    ses_handle h_ = nullptr;
+};
+
+struct Vec3d {
+    double x{}, y{}, z{};
+};
+
+// norm_sq(Field3D) (core/src/field.ixx:68-74): sum |psi|^2 dV, left to right
+inline double norm_sq(const Field3D& f) {
+    double s = 0.0;
+    for (const cd& v : f.data()) s += std::norm(v);
+    return s * f.grid().cell_volume();
+}
+
+// probability_density (core/src/field.ixx:100-106)
+inline std::vector<double> probability_density(const Field3D& f) {
+    std::vector<double> rho(f.data().size());
+    for (std::size_t i = 0; i < rho.size(); ++i) rho[i] = std::norm(f.data()[i]);
+    return rho;
+}
+
+// gaussian_wavepacket(Grid3D, r0, sigma, k0) (core/src/wavepacket.ixx:29-49):
+// separable Gaussian envelope (2 pi s^2)^(-1/4) exp(-(u - u0)^2 / (4 s^2)) per axis
+// times e^{i k0 . r}, then normalised so that norm_sq = 1.
+inline Field3D gaussian_wavepacket(const Grid3D& g, Vec3d r0, Vec3d sigma, Vec3d k0) {
+    constexpr double kPi = 3.14159265358979323846;
+    auto envelope = [](double u, double u0, double s) {
+        return std::pow(2.0 * kPi * s * s, -0.25) * std::exp(-(u - u0) * (u - u0) / (4.0 * s * s));
+    };
+    Field3D psi(g);
+    for (int k = 0; k < g.z.n; ++k)
+        for (int j = 0; j < g.y.n; ++j)
+            for (int i = 0; i < g.x.n; ++i) {
+                const double x = g.x.coord(i), y = g.y.coord(j), z = g.z.coord(k);
+                const double env = envelope(x, r0.x, sigma.x) * envelope(y, r0.y, sigma.y) * envelope(z, r0.z, sigma.z);
+                const double phase = k0.x * x + k0.y * y + k0.z * z;
+                psi(i, j, k) = cd{env * std::cos(phase), env * std::sin(phase)};
+            }
+    const double n2 = norm_sq(psi);
+    if (n2 > 0.0) {
+        const double inv = 1.0 / std::sqrt(n2);
+        for (cd& v : psi.data()) v *= inv;
+    }
+    return psi;
+}
+
+// WavepacketSimulation (core/src/simulation.ixx:22-88): Config -> tables and
+// psi0; advance(n) steps the field resident on the device, psi() / density()
+// read it back when it changed, set_psi() uploads a field, relax(n, dtau) runs
+// imaginary time on it.  The POVM measurement of the reference (measure) is not
+// part of the step and is not provided.
+class WavepacketSimulation {
+public:
+    struct Config {
+        Grid3D grid;
+        std::vector<double> potential;
+        Vec3d r0;
+        Vec3d sigma;
+        Vec3d k0;
+        double dt;
+    };
+
+    explicit WavepacketSimulation(Config cfg, ses_precision prec = SES_C128)
+        : grid_(cfg.grid),
+          dt_(cfg.dt),
+          prec_(prec),
+          potential_(std::move(cfg.potential)),
+          propagator_(cfg.grid, potential_, cfg.dt, 1.0, prec),
+          psi_(gaussian_wavepacket(cfg.grid, cfg.r0, cfg.sigma, cfg.k0)) {
+        propagator_.upload_state(psi_.data());
+    }
+
+    void advance(int nsteps) {
+        propagator_.advance(nsteps);
+        steps_ += nsteps;
+        stale_ = true;
+    }
+
+    // imaginary-time relaxation of the current field with step dtau (tau is not t)
+    void relax(int nsteps, double dtau) {
+        if (!relaxer_ || relaxer_dtau_ != dtau) {
+            relaxer_.reset(new ImaginaryTimePropagator3D(grid_, potential_, dtau, 1.0, prec_));
+            relaxer_dtau_ = dtau;
+        }
+        Field3D& p = current();
+        relaxer_->relax(p, nsteps);
+        propagator_.upload_state(p.data());
+    }
+
+    double time() const noexcept { return static_cast<double>(steps_) * dt_; }
+    double dt() const noexcept { return dt_; }
+    const Grid3D& grid() const noexcept { return grid_; }
+    const Field3D& psi() const { return current(); }
+    const std::vector<double>& potential() const noexcept { return potential_; }
+    const SplitOperator3D& propagator() const noexcept { return propagator_; }
+    SplitOperator3D& propagator() noexcept { return propagator_; }
+
+    void set_psi(const Field3D& psi) {
+        if (psi.size() != psi_.size()) throw std::invalid_argument("field does not match the grid");
+        psi_ = psi;
+        propagator_.upload_state(psi_.data());
+        stale_ = false;
+    }
+    std::vector<double> density() const { return probability_density(current()); }
+
+private:
+    Field3D& current() const {
+        if (stale_) {
+            psi_.data() = propagator_.readback();
+            stale_ = false;
+        }
+        return psi_;
+    }
+
+    Grid3D grid_;
+    double dt_;
+    ses_precision prec_;
+    std::vector<double> potential_;
+    SplitOperator3D propagator_;
+    mutable Field3D psi_;
+    mutable bool stale_ = false;
+    long long steps_ = 0;
+    std::unique_ptr<ImaginaryTimePropagator3D> relaxer_;
+    double relaxer_dtau_ = 0.0;
 };
 
 // SplitOperator1D (propagator.ixx:21-66): the 3D engine on n x 1 x 1
@@ -202,6 +370,7 @@ public:
     }
     std::size_t size() const noexcept { return members_.size(); }
     void step(int nsteps, bool absorb = false) { check(ses_batch_step(b_, nsteps, absorb ? 1 : 0)); }
+    void prepare(bool absorb = false) { check(ses_batch_prepare(b_, absorb ? 1 : 0)); }
     std::vector<ses_observables> observe(double xlo = -1e300, double xhi = 1e300) {
         std::vector<ses_observables> out(members_.size());
         check(ses_batch_observe(b_, xlo, xhi, out.data(), static_cast<int>(out.size())));

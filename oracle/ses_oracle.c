@@ -11,8 +11,10 @@
 #include "ses_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 typedef struct {
     double re, im;
@@ -136,6 +138,61 @@ static void fft_line(cplx* a, size_t n, const cplx* w, cplx* scratch) {
     memcpy(a, out, n * sizeof(cplx));
 }
 
+/* Worker threads for independent lines and elements.  Every line (element) is
+ * computed by the same serial code whichever thread runs it, so results are
+ * bit-identical to a single-threaded run -- the property the reference's
+ * deterministic pool guarantees (core/src/parallel.ixx:14-16).  SESO_THREADS
+ * sets the count (default: the online cores). */
+typedef void (*range_fn)(void* ctx, size_t begin, size_t end);
+
+enum { kMaxThreads = 256 };
+
+static int oracle_threads(void) {
+    const char* e = getenv("SESO_THREADS");
+    long t = e ? atol(e) : sysconf(_SC_NPROCESSORS_ONLN);
+    if (t < 1) t = 1;
+    if (t > kMaxThreads) t = kMaxThreads;
+    return (int)t;
+}
+
+typedef struct {
+    range_fn fn;
+    void* ctx;
+    size_t begin, end;
+} range_job;
+
+static void* run_range(void* p) {
+    range_job* j = (range_job*)p;
+    j->fn(j->ctx, j->begin, j->end);
+    return NULL;
+}
+
+/* fn over [0, count) in contiguous chunks; `work` = rough cost of the whole call in
+ * element operations, below which threads are not worth starting */
+static void par_for(size_t count, size_t work, range_fn fn, void* ctx) {
+    size_t t = (size_t)oracle_threads();
+    if (t > count) t = count;
+    if (t <= 1 || work < ((size_t)1 << 16)) {
+        fn(ctx, 0, count);
+        return;
+    }
+    pthread_t th[kMaxThreads];
+    range_job jobs[kMaxThreads];
+    int started[kMaxThreads];
+    for (size_t i = 0; i < t; ++i) {
+        jobs[i].fn = fn;
+        jobs[i].ctx = ctx;
+        jobs[i].begin = count * i / t;
+        jobs[i].end = count * (i + 1) / t;
+        started[i] = i > 0 && pthread_create(&th[i], NULL, run_range, &jobs[i]) == 0;
+    }
+    run_range(&jobs[0]);
+    for (size_t i = 1; i < t; ++i) {
+        if (started[i]) pthread_join(th[i], NULL);
+        else run_range(&jobs[i]);  /* a thread that could not start runs here */
+    }
+}
+
 static cplx* make_table(size_t n) {
     if (is_pow2(n)) {
         cplx* w = (cplx*)malloc((n / 2 + 1) * sizeof(cplx));
@@ -162,16 +219,47 @@ int seso_fft1d(double* a, size_t n) {
     return 0;
 }
 
+typedef struct {
+    cplx* a;
+    const cplx* ph;
+    const double* m;
+    double inv;
+} elem_ctx;
+
+static void conj_range(void* p, size_t b, size_t e) {
+    cplx* a = ((elem_ctx*)p)->a;
+    for (size_t i = b; i < e; ++i) a[i].im = -a[i].im;
+}
+
+static void conj_scale_range(void* p, size_t b, size_t e) {
+    const elem_ctx* c = (const elem_ctx*)p;
+    for (size_t i = b; i < e; ++i) {
+        c->a[i].re = c->inv * c->a[i].re;
+        c->a[i].im = c->inv * -c->a[i].im;
+    }
+}
+
+static void phase_range(void* p, size_t b, size_t e) {
+    const elem_ctx* c = (const elem_ctx*)p;
+    for (size_t i = b; i < e; ++i) c->a[i] = cmul(c->a[i], c->ph[i]);
+}
+
+static void mask_range(void* p, size_t b, size_t e) {
+    const elem_ctx* c = (const elem_ctx*)p;
+    for (size_t i = b; i < e; ++i) {
+        c->a[i].re *= c->m[i];
+        c->a[i].im *= c->m[i];
+    }
+}
+
 static void conj_all(cplx* a, size_t n) {
-    for (size_t i = 0; i < n; ++i) a[i].im = -a[i].im;
+    elem_ctx c = {a, NULL, NULL, 0.0};
+    par_for(n, n, conj_range, &c);
 }
 
 static void conj_scale_all(cplx* a, size_t n) {
-    const double inv = 1.0 / (double)n;
-    for (size_t i = 0; i < n; ++i) {
-        a[i].re = inv * a[i].re;
-        a[i].im = inv * -a[i].im;
-    }
+    elem_ctx c = {a, NULL, NULL, 1.0 / (double)n};
+    par_for(n, n, conj_scale_range, &c);
 }
 
 int seso_ifft1d(double* a, size_t n) {
@@ -182,43 +270,49 @@ int seso_ifft1d(double* a, size_t n) {
     return 0;
 }
 
-/* x lines in place, then y and z lines through a gathered scratch line */
-int seso_fft3d(double* data, const int* n) {
-    for (int ax = 0; ax < 3; ++ax)
-        if (seso_supported_length((size_t)n[ax]) != 0) return -1;
-    cplx* a = (cplx*)data;
-    const int nx = n[0], ny = n[1], nz = n[2];
-    int nmax = nx > ny ? nx : ny;
-    nmax = nmax > nz ? nmax : nz;
-    cplx* line = (cplx*)malloc((size_t)nmax * sizeof(cplx));
-    cplx* scr = (cplx*)malloc(2 * (size_t)nmax * sizeof(cplx));
-    if (nx > 1) {
-        cplx* w = make_table((size_t)nx);
-        for (int m = 0; m < ny * nz; ++m) fft_line(a + (size_t)m * nx, (size_t)nx, w, scr);
-        free(w);
-    }
-    if (ny > 1) {
-        cplx* w = make_table((size_t)ny);
-        for (int k = 0; k < nz; ++k)
-            for (int i = 0; i < nx; ++i) {
-                for (int j = 0; j < ny; ++j) line[j] = a[flat(n, i, j, k)];
-                fft_line(line, (size_t)ny, w, scr);
-                for (int j = 0; j < ny; ++j) a[flat(n, i, j, k)] = line[j];
-            }
-        free(w);
-    }
-    if (nz > 1) {
-        cplx* w = make_table((size_t)nz);
-        for (int j = 0; j < ny; ++j)
-            for (int i = 0; i < nx; ++i) {
-                for (int k = 0; k < nz; ++k) line[k] = a[flat(n, i, j, k)];
-                fft_line(line, (size_t)nz, w, scr);
-                for (int k = 0; k < nz; ++k) a[flat(n, i, j, k)] = line[k];
-            }
-        free(w);
+typedef struct {
+    cplx* a;
+    const int* n;
+    const cplx* w;
+    int axis;
+} lines_ctx;
+
+/* lines [begin, end) of one axis: x lines in place, y and z lines through a
+ * gathered scratch line */
+static void fft_lines(void* p, size_t begin, size_t end) {
+    const lines_ctx* c = (const lines_ctx*)p;
+    const int* n = c->n;
+    const int len = n[c->axis];
+    cplx* line = (cplx*)malloc((size_t)len * sizeof(cplx));
+    cplx* scr = (cplx*)malloc(2 * (size_t)len * sizeof(cplx));
+    for (size_t m = begin; m < end; ++m) {
+        if (c->axis == 0) {
+            fft_line(c->a + m * (size_t)n[0], (size_t)len, c->w, scr);
+            continue;
+        }
+        /* y: line m = (i, k) with m = i + nx k; z: line m = (i, j) with m = i + nx j */
+        const int i = (int)(m % (size_t)n[0]), o = (int)(m / (size_t)n[0]);
+        for (int e = 0; e < len; ++e) line[e] = c->a[c->axis == 1 ? flat(n, i, e, o) : flat(n, i, o, e)];
+        fft_line(line, (size_t)len, c->w, scr);
+        for (int e = 0; e < len; ++e) c->a[c->axis == 1 ? flat(n, i, e, o) : flat(n, i, o, e)] = line[e];
     }
     free(scr);
     free(line);
+}
+
+/* Forward unnormalised 3D transform: all x lines, then all y lines, then all z
+ * lines (core/src/fft.ixx:102-173). */
+int seso_fft3d(double* data, const int* n) {
+    for (int ax = 0; ax < 3; ++ax)
+        if (seso_supported_length((size_t)n[ax]) != 0) return -1;
+    const size_t N = total(n);
+    for (int ax = 0; ax < 3; ++ax) {
+        if (n[ax] <= 1) continue;
+        cplx* w = make_table((size_t)n[ax]);
+        lines_ctx c = {(cplx*)data, n, w, ax};
+        par_for(N / (size_t)n[ax], N * 8, fft_lines, &c);
+        free(w);
+    }
     return 0;
 }
 
@@ -292,7 +386,8 @@ void seso_tables3d(const double* box, const int* n, const double* V, double dt, 
 }
 
 static void apply_phase(cplx* a, const cplx* ph, size_t N) {
-    for (size_t i = 0; i < N; ++i) a[i] = cmul(a[i], ph[i]);
+    elem_ctx c = {a, ph, NULL, 0.0};
+    par_for(N, N, phase_range, &c);
 }
 
 int seso_step3d(const double* box, const int* n, const double* V, double dt, double mass,
@@ -311,10 +406,8 @@ int seso_step3d(const double* box, const int* n, const double* V, double dt, dou
         seso_ifft3d(psi, n);
         apply_phase(a, half, N);
         if (mask) {
-            for (size_t i = 0; i < N; ++i) {
-                a[i].re *= mask[i];
-                a[i].im *= mask[i];
-            }
+            elem_ctx c = {a, NULL, mask, 0.0};
+            par_for(N, N, mask_range, &c);
         }
     }
     free(half);

@@ -1,8 +1,10 @@
 """ctypes binding of the C ABI in include/ses_gpu.h (libses_b200.so).
 
-The library is built in-tree (``python shoeridingerequationsolver_b200/build.py``).
-There is no fallback: if the shared library is missing or fails to load,
-importing this module raises ``ImportError``.
+The library is built in-tree (``python shoeridingerequationsolver_b200/build.py``)
+and mapped on the first call that needs it (creating a handle, a batch, a
+server, an FFT, a device count): importing the package to build host arrays
+(``scenes``) does not map it.  There is no fallback: if the shared library is
+missing or fails to load, that first call raises ``ImportError``.
 """
 
 from __future__ import annotations
@@ -29,7 +31,8 @@ EXPORTS = [
     "ses_serve_open", "ses_serve_submit", "ses_serve_poll", "ses_serve_result", "ses_serve_cancel",
     "ses_serve_wait_idle", "ses_serve_stats", "ses_serve_close", "ses_gpu_create_imag", "ses_gpu_relax",
     "ses_gpu_step_driven", "ses_gpu_snapshot", "ses_gpu_restore", "ses_gpu_density_slice",
-    "ses_batch_observe_some", "ses_batch_run",
+    "ses_batch_observe_some", "ses_batch_run", "ses_gpu_norm_and_peak", "ses_gpu_scale", "ses_gpu_prepare",
+    "ses_batch_prepare", "ses_gpu_set_wait_limit",
 ]
 
 
@@ -122,6 +125,11 @@ def _load() -> C.CDLL:
         "ses_gpu_set_stream": ([hp, vp], st),
         "ses_gpu_psi_device": ([hp, C.POINTER(vp), C.POINTER(C.c_size_t)], st),
         "ses_gpu_footprint": ([hp, C.POINTER(C.c_size_t)], st),
+        "ses_gpu_norm_and_peak": ([hp, dp, dp], st),
+        "ses_gpu_scale": ([hp, C.c_double], st),
+        "ses_gpu_prepare": ([hp, C.c_int], st),
+        "ses_batch_prepare": ([vp, C.c_int], st),
+        "ses_gpu_set_wait_limit": ([hp, C.c_int64, C.c_uint32], st),
         "ses_fft3_host": ([C.POINTER(C.c_int32), C.c_int, dp, C.c_int], st),
         "ses_gpu_profile_step": ([hp, C.c_int, C.c_int, dp], st),
         "ses_gpu_autotune": ([hp, C.c_int], st),
@@ -160,7 +168,27 @@ def _load() -> C.CDLL:
     return lib
 
 
-lib = _load()
+class _LazyLib:
+    """Stands for the CDLL of libses_b200.so and maps it on first attribute use."""
+
+    _cdll: C.CDLL | None = None
+
+    def __getattr__(self, name):
+        if _LazyLib._cdll is None:
+            _LazyLib._cdll = _load()
+        return getattr(_LazyLib._cdll, name)
+
+    @staticmethod
+    def loaded() -> bool:
+        return _LazyLib._cdll is not None
+
+
+lib = _LazyLib()
+
+
+def ensure_loaded() -> None:
+    """Map the library now (raises ImportError when it is not built)."""
+    lib.ses_version  # noqa: B018  (attribute access maps the library)
 
 
 def last_error() -> str:

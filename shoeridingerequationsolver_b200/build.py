@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libses_b200.so"
 SOURCES = ["ses_gpu.cu", "ses_plans_small.cu", "ses_plans_mixed.cu", "ses_plans_256.cu",
            "ses_plans_large.cu", "ses_noalloc.cu", "ses_serve.cpp"]
-HEADERS = ["ses_fft.cuh", "ses_pass.cuh", "ses_pass2.cuh", "ses_pass3.cuh", "ses_tma.cuh", "ses_plans.cuh",
+HEADERS = ["ses_fft.cuh", "ses_pass.cuh", "ses_pass2.cuh", "ses_pass3.cuh", "ses_tma.cuh", "ses_plans.cuh", "ses_engine.cuh",
            "ses_aux.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -40,16 +40,36 @@ def up_to_date() -> bool:
     return all(d.stat().st_mtime <= t for d in deps)
 
 
+def includes(path: Path, seen=None) -> set:
+    """The quoted #include files of a source, followed recursively inside csrc/ and include/."""
+    seen = set() if seen is None else seen
+    for line in path.read_text().splitlines():
+        line = line.strip()
+        if not line.startswith('#include "'):
+            continue
+        name = line.split('"')[1]
+        for d in (CSRC, ROOT / "include"):
+            f = d / name
+            if f.exists() and f not in seen:
+                seen.add(f)
+                includes(f, seen)
+    return seen
+
+
 def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
-    """Compile each translation unit in parallel, then link the shared library."""
+    """Compile each out-of-date translation unit in parallel, then link the shared library."""
     if not force and up_to_date():
         return LIB
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
     compile_flags = [f for f in FLAGS if f != "-shared"]
-    procs = []
+    procs, objs = [], []
     for src in SOURCES:
         obj = objdir / (Path(src).stem + ".o")
+        objs.append(obj)
+        deps = [CSRC / src, Path(__file__), *includes(CSRC / src)]
+        if not force and obj.exists() and all(d.stat().st_mtime <= obj.stat().st_mtime for d in deps):
+            continue
         cmd = [nvcc(), *ARCH, *compile_flags, "-I", str(ROOT / "include"), "-I", str(CSRC), "-c",
                str(CSRC / src), "-o", str(obj)]
         if ptxas_verbose:
@@ -58,7 +78,7 @@ def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
     failed = [str(o) for o, p in procs if p.wait() != 0]
     if failed:
         raise RuntimeError(f"nvcc failed for {failed}")
-    link = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *[str(o) for o, _ in procs], "-o", str(LIB)]
+    link = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *[str(o) for o in objs], "-o", str(LIB)]
     subprocess.run(link, check=True)
     return LIB
 

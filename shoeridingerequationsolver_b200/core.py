@@ -310,6 +310,26 @@ class SplitOperator3D:
     def sync(self, timeout_ms: int = 0) -> None:
         check(lib.ses_gpu_sync(self._h, int(timeout_ms)))
 
+    def norm_and_peak(self) -> tuple[float, float]:
+        """Engine::norm_and_peak (vk_engine.ixx:1665-1692): (sum |psi|^2 dV, max |psi|^2)."""
+        nrm, peak = C.c_double(), C.c_double()
+        check(lib.ses_gpu_norm_and_peak(self._h, C.byref(nrm), C.byref(peak)))
+        return nrm.value, peak.value
+
+    def scale(self, factor: float) -> None:
+        """Engine::scale (vk_engine.ixx:2120-2133): psi <- factor * psi on the device."""
+        check(lib.ses_gpu_scale(self._h, float(factor)))
+
+    def prepare(self, absorb: bool = False) -> None:
+        """Record the step graph now (not inside the first long advance)."""
+        check(lib.ses_gpu_prepare(self._h, 1 if absorb else 0))
+
+    def set_wait_limit(self, wait_cycles: int = 0, extra_tx_bytes: int = 0) -> None:
+        """Failure-detection hook (ses_gpu_set_wait_limit): bound the pipelined passes'
+        waits by wait_cycles SM cycles and, with extra_tx_bytes > 0, make every tile's
+        wait run out; (0, 0) restores normal operation."""
+        check(lib.ses_gpu_set_wait_limit(self._h, int(wait_cycles), int(extra_tx_bytes)))
+
     def set_stream(self, stream_ptr: int | None) -> None:
         check(lib.ses_gpu_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
 
@@ -423,6 +443,117 @@ class ImaginaryTimePropagator3D(SplitOperator3D):
         return e.value
 
 
+def gaussian_wavepacket(grid: Grid3D, r0, sigma, k0) -> Field3D:
+    """gaussian_wavepacket(Grid3D, r0, sigma, k0) (core/src/wavepacket.ixx:29-49):
+    per-axis envelope (2 pi s^2)^(-1/4) exp(-(u - u0)^2 / (4 s^2)) times
+    e^{i k0 . r}, normalised to norm_sq = 1 on the grid."""
+    def env(u, u0, s):
+        return math.pow(2.0 * math.pi * s * s, -0.25) * np.exp(-(u - u0) * (u - u0) / (4.0 * s * s))
+    x = grid.x.coords()[None, None, :]
+    y = grid.y.coords()[None, :, None]
+    z = grid.z.coords()[:, None, None]
+    amp = env(x, r0[0], sigma[0]) * env(y, r0[1], sigma[1]) * env(z, r0[2], sigma[2])
+    ph = k0[0] * x + k0[1] * y + k0[2] * z
+    psi = (amp * np.cos(ph) + 1j * (amp * np.sin(ph))).reshape(-1)
+    n2 = float(np.sum(psi.real * psi.real + psi.imag * psi.imag)) * grid.cell_volume()
+    if n2 > 0.0:
+        psi = psi / math.sqrt(n2)
+    return Field3D(grid, psi)
+
+
+@dataclass
+class SimulationConfig:
+    """WavepacketSimulation::Config (core/src/simulation.ixx:24-31)."""
+    grid: Grid3D
+    potential: np.ndarray
+    r0: tuple
+    sigma: tuple
+    k0: tuple
+    dt: float
+
+
+class WavepacketSimulation:
+    """WavepacketSimulation (core/src/simulation.ixx:22-88) on the B200.
+
+    The config builds the propagator tables (on the device) and psi0 =
+    gaussian_wavepacket(grid, r0, sigma, k0); psi stays resident in HBM.
+    ``advance(n)`` steps it there; ``psi()`` / ``density()`` read it back when it
+    changed; ``set_psi`` uploads a field (the reference's hook for injecting a
+    GPU-evolved field); ``relax(n, dtau)`` runs imaginary time on it.  The POVM
+    ``measure`` of the reference is not part of the step and is not provided."""
+
+    Config = SimulationConfig
+
+    def __init__(self, cfg: SimulationConfig, precision: str = "c128"):
+        self._grid = cfg.grid
+        self._dt = float(cfg.dt)
+        self._precision = precision
+        self._potential = np.ascontiguousarray(np.asarray(cfg.potential, dtype=np.float64).reshape(-1))
+        self._prop = SplitOperator3D(cfg.grid, self._potential, cfg.dt, precision=precision)
+        self._psi = gaussian_wavepacket(cfg.grid, cfg.r0, cfg.sigma, cfg.k0)
+        self._prop.upload_state(self._psi.data)
+        self._stale = False
+        self._steps = 0
+        self._relaxer = None
+        self._relaxer_dtau = 0.0
+
+    def advance(self, nsteps: int) -> None:
+        self._prop.advance(int(nsteps))
+        self._steps += int(nsteps)
+        self._stale = True
+
+    def relax(self, nsteps: int, dtau: float) -> None:
+        if self._relaxer is None or self._relaxer_dtau != dtau:
+            if self._relaxer is not None:
+                self._relaxer.close()
+            self._relaxer = ImaginaryTimePropagator3D(self._grid, self._potential, dtau,
+                                                      precision=self._precision)
+            self._relaxer_dtau = dtau
+        f = self.psi()
+        self._relaxer.relax(f, int(nsteps))
+        self._prop.upload_state(f.data)
+
+    def time(self) -> float:
+        return self._steps * self._dt
+
+    def dt(self) -> float:
+        return self._dt
+
+    def grid(self) -> Grid3D:
+        return self._grid
+
+    def potential(self) -> np.ndarray:
+        return self._potential
+
+    def propagator(self) -> SplitOperator3D:
+        return self._prop
+
+    def psi(self) -> Field3D:
+        if self._stale:
+            self._prop.readback(out=self._psi.data)
+            self._stale = False
+        return self._psi
+
+    def set_psi(self, psi: Field3D) -> None:
+        data = psi.data if isinstance(psi, Field3D) else np.asarray(psi)
+        if data.size != self._grid.size():
+            raise ValueError("field size does not match the grid")
+        self._psi = Field3D(self._grid, data)
+        self._prop.upload_state(self._psi.data)
+        self._stale = False
+
+    def density(self) -> np.ndarray:
+        """probability_density (core/src/field.ixx:100-106): |psi|^2 per cell."""
+        d = self.psi().data
+        return d.real * d.real + d.imag * d.imag
+
+    def close(self) -> None:
+        self._prop.close()
+        if self._relaxer is not None:
+            self._relaxer.close()
+            self._relaxer = None
+
+
 class SplitOperator1D:
     """1D Strang propagator (propagator.ixx:21-66): the 3D engine on n x 1 x 1."""
 
@@ -478,6 +609,10 @@ class Batch:
 
     def step(self, nsteps: int, absorb: bool = False) -> None:
         check(lib.ses_batch_step(self._b, int(nsteps), 1 if absorb else 0))
+
+    def prepare(self, absorb: bool = False) -> None:
+        """Record every class's step graph now (ses_batch_prepare)."""
+        check(lib.ses_batch_prepare(self._b, 1 if absorb else 0))
 
     def observe(self, xlo: float = -math.inf, xhi: float = math.inf) -> list[dict]:
         n = len(self._members)

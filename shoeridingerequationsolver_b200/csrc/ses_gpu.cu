@@ -22,6 +22,7 @@
 
 #include "ses_gpu.h"
 #include "ses_aux.cuh"
+#include "ses_engine.cuh"
 #include "ses_pass.cuh"
 #include "ses_plans.cuh"
 
@@ -261,6 +262,8 @@ struct ses_solver {
     int sms = 148;
     bool pipelined = true;
     bool pdl = true;  // single-field passes launched with programmatic stream serialization
+    long long wait_limit = 0;      // failure-detection hook: bounded-wait limit of pipelined passes (0: ~2 s)
+    uint32_t extra_tx = 0;         // failure-detection hook: bytes each tile barrier expects beyond its copies
     int xsel = 0;                  // pipelined contiguous-pass variant (-1: register path)
     int ssel[3] = {0, 0, 0};       // pipelined strided-pass variant per axis (-1: register path)
     ses_batch_s* batch = nullptr;  // batch this handle belongs to (its stream is the batch's)
@@ -467,6 +470,8 @@ ses_status launch(const ses_solver* h, int axis, int mode, const PassArgs<T>& a,
             PipeArgs pa{};
             pa.ntiles = (int)((pp.nlines + v.lpc - 1) / v.lpc);
             pa.err = h->derr;
+            pa.wait_limit = h->wait_limit;
+            pa.extra_tx = h->extra_tx;
             const int grid = std::min(pa.ntiles, h->sms * v.bps[mode]);
             launch_pass(h->pdl, v.k[mode], (unsigned)grid, 32u * v.warps, v.smem[mode], s, a, pa);
             done = true;
@@ -483,6 +488,8 @@ ses_status launch(const ses_solver* h, int axis, int mode, const PassArgs<T>& a,
                 pa.rows_per_box = n > 256 ? 256 : n;
                 pa.nbox = n / pa.rows_per_box;
                 pa.err = h->derr;
+                pa.wait_limit = h->wait_limit;
+                pa.extra_tx = h->extra_tx;
                 const int grid = std::min(pa.ntiles, h->sms * v.bps[mode]);
                 launch_pass(h->pdl, v.k[mode], (unsigned)grid, (unsigned)(v.ls * tl), v.smem, s, a,
                             h->tmap[buf][axis][ss], pa);
@@ -745,9 +752,37 @@ ses_status enqueue_driven(ses_solver* h, int S, bool mask, const double* axis, d
     return pass_x<T>(h, h->psi, h->psi, end, s);
 }
 
+// Natural-order transform of a long 1D line x[n1 + N1 n2] (fft(std::vector<cd>&),
+// core/src/fft.ixx:75-98).  Four steps: the strided pass transforms over n2 and
+// multiplies by W_N^{n1 k2}, the contiguous pass transforms over n1, leaving
+// X[k2 + N2 k1] at k1 + N1 k2; a transpose through the scratch field puts it in
+// natural order.  The inverse conjugates around the forward transform
+// (fft.ixx:89-98): conj(fft(conj(X))) / N.
+template <typename T>
+ses_status enqueue_fft_long(ses_solver* h, int inverse) {
+    cudaStream_t s = h->stream;
+    cx<T>* psi = reinterpret_cast<cx<T>*>(h->psi);
+    const unsigned eb = (unsigned)std::min<long long>((h->N + 255) / 256, (long long)h->sms * 8);
+    if (inverse) scale_kernel<T><<<eb, 256, 0, s>>>(psi, h->N, 1.0, 1);
+    XProg none;
+    SES_TRY(pass_tw<T>(h, h->psi, h->psi, SM_TW_START, none, s));
+    XProg fwd;
+    fwd.mode = XM_FWD;
+    SES_TRY(pass_x<T>(h, h->psi, h->psi, fwd, s));
+    const int n1 = h->n[0], n2 = h->n[1];
+    transpose_kernel<T><<<dim3((unsigned)(n1 + 31) / 32, (unsigned)(n2 + 31) / 32), dim3(32, 8), 0, s>>>(
+        psi, reinterpret_cast<cx<T>*>(h->scratch), n2, n1);
+    SES_CU(cudaGetLastError());
+    SES_CU(cudaMemcpyAsync(h->psi, h->scratch, (size_t)h->N * sizeof(cx<T>), cudaMemcpyDeviceToDevice, s));
+    if (inverse) scale_kernel<T><<<eb, 256, 0, s>>>(psi, h->N, 1.0 / (double)h->N, 1);
+    SES_CU(cudaGetLastError());
+    return SES_OK;
+}
+
 template <typename T>
 ses_status enqueue_fft3(ses_solver* h, void* data, int inverse) {
     cudaStream_t s = h->stream;
+    if (h->long1d) return enqueue_fft_long<T>(h, inverse);
     if (!inverse) {
         XProg p;
         p.mode = XM_FWD;
@@ -2255,9 +2290,6 @@ ses_status ses_gpu_step_driven(ses_handle h, int nsteps, int absorb, const doubl
 ses_status ses_gpu_fft3(ses_handle h, int direction) {
     SES_TRY(check_handle(h));
     if (direction != 0 && direction != 1) return fail(SES_EINVAL, "direction must be 0 or 1");
-    if (h->long1d)
-        return fail(SES_EINVAL, "lines above 4096 points are transformed only inside the step (four-step "
-                                "layout); no natural-order FFT of them");
     return h->prec == SES_C128 ? enqueue_fft3<double>(h, h->psi, direction)
                                : enqueue_fft3<float>(h, h->psi, direction);
 }
@@ -2451,6 +2483,55 @@ ses_status ses_gpu_footprint(ses_handle h, size_t* bytes) {
     return SES_OK;
 }
 
+ses_status ses_gpu_norm_and_peak(ses_handle h, double* norm, double* peak) {
+    SES_TRY(check_handle(h));
+    if (!norm && !peak) return fail(SES_EINVAL, "null outputs");
+    cudaStream_t s = h->stream;
+    if (h->prec == SES_C128)
+        norm_peak_kernel<double><<<kNormPeakBlocks, 256, 0, s>>>(reinterpret_cast<const cx<double>*>(h->psi), h->N,
+                                                                 h->partials);
+    else
+        norm_peak_kernel<float><<<kNormPeakBlocks, 256, 0, s>>>(reinterpret_cast<const cx<float>*>(h->psi), h->N,
+                                                                h->partials);
+    norm_peak_finalize<<<1, 32, 0, s>>>(h->partials, kNormPeakBlocks, h->dsums);
+    SES_CU(cudaGetLastError());
+    SES_CU(cudaMemcpyAsync(h->hsums, h->dsums, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    SES_TRY(wait_bounded(h, 0));
+    const double dv = ((h->box[1] - h->box[0]) / phys_n(h, 0)) * ((h->box[3] - h->box[2]) / phys_n(h, 1)) *
+                      ((h->box[5] - h->box[4]) / phys_n(h, 2));
+    if (norm) *norm = h->hsums[0] * dv;
+    if (peak) *peak = h->hsums[1];
+    return SES_OK;
+}
+
+ses_status ses_gpu_scale(ses_handle h, double factor) {
+    SES_TRY(check_handle(h));
+    if (!std::isfinite(factor)) return fail(SES_EINVAL, "scale factor must be finite");
+    const unsigned eb = (unsigned)std::min<long long>((h->N + 255) / 256, (long long)h->sms * 8);
+    if (h->prec == SES_C128)
+        scale_kernel<double><<<eb, 256, 0, h->stream>>>(reinterpret_cast<cx<double>*>(h->psi), h->N, factor, 0);
+    else
+        scale_kernel<float><<<eb, 256, 0, h->stream>>>(reinterpret_cast<cx<float>*>(h->psi), h->N, factor, 0);
+    SES_CU(cudaGetLastError());
+    return SES_OK;
+}
+
+ses_status ses_gpu_set_wait_limit(ses_handle h, int64_t wait_cycles, uint32_t extra_tx_bytes) {
+    SES_TRY(check_handle(h));
+    if (wait_cycles < 0) return fail(SES_EINVAL, "wait_cycles must be >= 0");
+    if (extra_tx_bytes > 4096) return fail(SES_EINVAL, "extra_tx_bytes must be <= 4096");
+    SES_TRY(wait_bounded(h, 0));  // launches already queued keep their limits
+    h->wait_limit = wait_cycles;
+    h->extra_tx = extra_tx_bytes;
+    drop_graphs(h);               // captured launches carry the old values
+    return SES_OK;
+}
+
+ses_status ses_gpu_prepare(ses_handle h, int absorb) {
+    SES_TRY(check_handle(h));
+    return h->prec == SES_C128 ? ensure_body<double>(h, absorb != 0) : ensure_body<float>(h, absorb != 0);
+}
+
 ses_status ses_fft3_host(const int32_t* n, ses_precision prec, double* data, int inverse) {
     if (!n || !data) return fail(SES_EINVAL, "null argument");
     ses_grid_desc g{};
@@ -2569,6 +2650,21 @@ ses_status ses_batch_step(ses_batch b, int nsteps, int absorb) {
                                     : class_steps<float>(b, *c, nsteps, mask, c->cs));
         SES_CU(cudaEventRecord(c->done, c->cs));
         SES_CU(cudaStreamWaitEvent(b->stream, c->done, 0));
+    }
+    return SES_OK;
+}
+
+ses_status ses_batch_prepare(ses_batch b, int absorb) {
+    SES_TRY(check_batch(b));
+    if (b->members.empty()) return SES_OK;
+    SES_TRY(batch_refresh(b));
+    for (BatchClass* c : b->classes) {
+        if (c->mem.empty()) continue;
+        if (!c->batched) {
+            for (ses_solver* h : c->mem) SES_TRY(ses_gpu_prepare(h, absorb));
+            continue;
+        }
+        SES_TRY(c->prec == SES_C128 ? class_body<double>(b, *c, absorb != 0) : class_body<float>(b, *c, absorb != 0));
     }
     return SES_OK;
 }

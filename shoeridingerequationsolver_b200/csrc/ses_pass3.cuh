@@ -19,6 +19,11 @@ struct PipeArgs {
     int rows_per_box;   // <= 256
     int nbox;           // boxes per tile along the transformed axis
     unsigned* err;      // device error word (bit 0: a bounded wait expired)
+    // failure-detection test hook (0 in normal launches): bounded-wait limit in SM
+    // cycles (0: ~2 s) and bytes every tile's barrier expects beyond what its copies
+    // deliver, so that the wait for it runs out; no copy is changed
+    long long wait_limit;
+    uint32_t extra_tx;
 };
 
 // Offset of the stage-twiddle copy: after the NBUF ring buffers and their
@@ -45,7 +50,7 @@ __device__ __forceinline__ void pipe_abort(const PipeArgs& pa, const uint64_t* b
                                            int nmine) {
     if (threadIdx.x == 0) atomicOr(pa.err, 1u);
     for (int j = i; j < nmine && j < i + nbuf; ++j)
-        (void)mbar_wait(smem_u32(&bars[j % nbuf]), (uint32_t)((j / nbuf) & 1));
+        (void)mbar_wait(smem_u32(&bars[j % nbuf]), (uint32_t)((j / nbuf) & 1), pa.wait_limit);
 }
 
 // Where a pipelined pass finds the tile with global index t (t walks
@@ -110,7 +115,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
         const CUtensorMap* map = f.tmap(t);
         const uint32_t bar = smem_u32(&bars[buf]);
         const uint32_t dst = smem_u32(tiles + (size_t)buf * N * L);
-        mbar_expect_tx(bar, TILE_BYTES);
+        mbar_expect_tx(bar, TILE_BYTES + pa.extra_tx);
         for (int bx = 0; bx < pa.nbox; ++bx) {
             const uint32_t d = dst + (uint32_t)(bx * pa.rows_per_box * L * (int)sizeof(cx<T>));
             if (pa.kind == 0)
@@ -124,7 +129,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
 
     for (int i = 0; i < nmine; ++i) {
         const int buf = i % NBUF;
-        const bool ok = mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i / NBUF) & 1));
+        const bool ok = mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i / NBUF) & 1), pa.wait_limit);
         if (__syncthreads_or(!ok)) {
             pipe_abort(pa, bars, NBUF, i, nmine);
             return;
@@ -282,7 +287,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
         const uint32_t bar = smem_u32(&bars[buf]);
         const uint32_t dst = smem_u32(smraw3 + (size_t)buf * BUF_BYTES);
         const bool sepm = kMrowRing && a.tb.maskfull == nullptr && a.tb.mask1[0] != nullptr;
-        mbar_expect_tx(bar, (kTab ? 2 * bytes : bytes) + (sepm ? MROW_BYTES : 0u));
+        mbar_expect_tx(bar, (kTab ? 2 * bytes : bytes) + (sepm ? MROW_BYTES : 0u) + pa.extra_tx);
         bulk_g2s(dst, a.src + m0 * N, bytes, bar);
         if constexpr (kTab) bulk_g2s(dst + PSI_BYTES, vtab + m0 * N, bytes, bar);
         if constexpr (kMrowRing)
@@ -293,7 +298,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
 
     for (int i = 0; i < nmine; ++i) {
         const int buf = i % NBUF;
-        const bool ok = mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i / NBUF) & 1));
+        const bool ok = mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i / NBUF) & 1), pa.wait_limit);
         if (__syncthreads_or(!ok)) {
             pipe_abort(pa, bars, NBUF, i, nmine);
             return;

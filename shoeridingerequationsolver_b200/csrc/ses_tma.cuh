@@ -52,12 +52,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 
 constexpr long long kWaitLimitCycles = 4000000000LL;  // ~2 s at the B200's SM clock
 
-// Wait until phase `parity` of the barrier completes, at most ~2 s.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Wait until phase `parity` of the barrier completes, at most `limit` SM clock
+// cycles (<= 0: ~2 s).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit = 0) {
     if (mbar_try_wait(bar, parity)) return true;
+    const long long lim = limit > 0 ? limit : kWaitLimitCycles;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > kWaitLimitCycles) return false;
+        if (clock64() - t0 > lim) return false;
     }
     return true;
 }

@@ -179,12 +179,30 @@ def config_c3(n: int = 512) -> Workload:
     (seeded), packet sigma 3 at x=-20 with k0 = (3,0,0), cos^(1/8) absorber on the
     outer 8%, dt 0.002, 500 steps, transmitted P(x >= 1) every 50 steps."""
     g = cube_grid(-60.0, 60.0, n)
-    rng = np.random.default_rng(SEED_BASE + 2)
-    v0 = float(rng.uniform(1.0, 5.0))
+    v0 = config_c3_meta()
     return Workload(f"c3_tunnel_{n}", g, barrier(g, v0, -1.0, 1.0),
                     gaussian(g, (-20.0, 0.0, 0.0), (3.0, 3.0, 3.0), (3.0, 0.0, 0.0)), 0.002, 500,
                     mask=mask_profiles(g, 0.08), observe_every=50, x_range=(1.0, math.inf),
                     meta={"seed": SEED_BASE + 2, "barrier_height": v0})
+
+
+def config_c3_strip(x0: float = -20.0) -> Workload:
+    """C3's scene on a 512 x 64 x 64 grid of the same spacing (transverse box
+    [-7.5, 7.5)): same barrier, packet (centred at x0), absorber, dt and step
+    count -- the reduced size on which the full 500-step run is checked."""
+    full_h = config_c3_meta()
+    gx = Grid1D(-60.0, 60.0, 512)
+    gt = Grid1D(-7.5, 7.5, 64)
+    g = Grid3D(gx, gt, gt)
+    psi0 = gaussian(g, (x0, 0.0, 0.0), (3.0, 3.0, 3.0), (3.0, 0.0, 0.0))
+    return Workload(f"c3_strip_512x64x64_x0_{x0:g}", g, barrier(g, full_h, -1.0, 1.0), psi0, 0.002, 500,
+                    mask=mask_profiles(g, 0.08), observe_every=50, x_range=(1.0, math.inf),
+                    meta={"seed": SEED_BASE + 2, "barrier_height": full_h, "x0": x0})
+
+
+def config_c3_meta() -> float:
+    """C3's seeded barrier height U[1, 5]."""
+    return float(np.random.default_rng(SEED_BASE + 2).uniform(1.0, 5.0))
 
 
 C4_SIZES = (32, 48, 64, 96, 128, 160)
@@ -217,6 +235,19 @@ def build_c4_instance(spec: dict) -> Workload:
     return Workload(f"c4_tunnel_{spec['n']}_{spec['index']}", g, barrier(g, spec["barrier"], -1.0, 1.0),
                     psi0, spec["dt"], spec["steps"], mask=mask_profiles(g, spec["mask_frac"]),
                     observe_every=100, x_range=(1.0, math.inf), meta=dict(spec))
+
+
+def build_c4_plane(spec: dict) -> Workload:
+    """The scene of a batched-sweep instance on one z-plane (n x n x 1)."""
+    half = 0.5 * spec["side"]
+    a = Grid1D(-half, half, spec["n"])
+    g = Grid3D(a, a, Grid1D(0.0, 1.0, 1))
+    s = spec["sigma"]
+    psi0 = gaussian(g, (-0.5 * half, 0.0, 0.0), (s, s, s), (spec["k0"], 0.0, 0.0))
+    mx, my, _ = mask_profiles(g, spec["mask_frac"])
+    return Workload(f"c4_plane_{spec['n']}_{spec['index']}", g, barrier(g, spec["barrier"], -1.0, 1.0), psi0,
+                    spec["dt"], spec["steps"], mask=(mx, my, np.ones(1)), observe_every=100,
+                    x_range=(1.0, math.inf), meta=dict(spec))
 
 
 def config_c5_specs(count: int = 48, seed: int = SEED_BASE + 4) -> list[dict]:

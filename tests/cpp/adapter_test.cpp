@@ -157,6 +157,54 @@ int main() {
         }
         EXPECT(threw, "batch run rejects a field of the wrong size");
     }
+    {  // simulation_test.cpp: WavepacketSimulation on 16^3 harmonic, r0 (2,0,0), k0 (0,0.5,0), dt 0.02
+        const double box[6] = {-8, 8, -8, 8, -8, 8};
+        const int n[3] = {16, 16, 16};
+        const double c[3] = {0, 0, 0}, r0[3] = {2, 0, 0}, sg[3] = {1, 1, 1}, k0[3] = {0, 0.5, 0};
+        std::vector<double> V(4096);
+        seso_harmonic3d(box, n, 1.0, c, V.data());
+        const ses::gpu::Grid3D g{{-8, 8, 16}, {-8, 8, 16}, {-8, 8, 16}};
+        ses::gpu::WavepacketSimulation sim{ses::gpu::WavepacketSimulation::Config{
+            g, V, ses::gpu::Vec3d{2, 0, 0}, ses::gpu::Vec3d{1, 1, 1}, ses::gpu::Vec3d{0, 0.5, 0}, 0.02}};
+        EXPECT(sim.time() == 0.0, "simulation time starts at 0");
+        std::vector<cd> manual(4096);
+        seso_gaussian3d(box, n, r0, sg, k0, reinterpret_cast<double*>(manual.data()));
+        double d0 = 0;  // host builder vs the oracle's (bit-pinned to the reference's)
+        for (int i = 0; i < 4096; ++i) d0 = std::fmax(d0, std::abs(sim.psi().data()[i] - manual[i]));
+        EXPECT(d0 < 1e-15, "gaussian_wavepacket matches the reference builder");
+        sim.advance(3);
+        sim.advance(2);
+        EXPECT(std::fabs(sim.time() - 5 * 0.02) < 1e-15, "time advances by steps x dt");
+        seso_step3d(box, n, V.data(), 0.02, 1.0, nullptr, reinterpret_cast<double*>(manual.data()), 5);
+        double md = 0;  // MatchesManualPropagation
+        for (int i = 0; i < 4096; ++i) {
+            md = std::fmax(md, std::fabs(sim.psi().data()[i].real() - manual[i].real()));
+            md = std::fmax(md, std::fabs(sim.psi().data()[i].imag() - manual[i].imag()));
+        }
+        std::printf("  simulation vs manual propagation: max diff %.3e\n", md);
+        EXPECT(md < 1e-13, "simulation matches manual propagation");
+        const std::vector<double> rho = sim.density();
+        double dd = 0;
+        for (int i = 0; i < 4096; ++i) dd = std::fmax(dd, std::fabs(rho[i] - std::norm(sim.psi().data()[i])));
+        EXPECT(dd == 0.0, "density is |psi|^2");
+        EXPECT(std::fabs(ses::gpu::norm_sq(sim.psi()) - 1.0) < 1e-12, "simulation conserves norm");
+        // Engine::norm_and_peak and scale on the resident field
+        const auto np = sim.propagator().norm_and_peak();
+        double peak = 0;
+        for (double r : rho) peak = std::fmax(peak, r);
+        EXPECT(std::fabs(np.sum - ses::gpu::norm_sq(sim.psi())) < 1e-13, "norm_and_peak sum");
+        EXPECT(std::fabs(np.peak - peak) <= 1e-15 * peak, "norm_and_peak peak");
+        sim.propagator().scale(0.5);
+        const auto np2 = sim.propagator().norm_and_peak();
+        EXPECT(std::fabs(np2.sum - 0.25 * np.sum) < 1e-13, "scale multiplies psi");
+        sim.propagator().scale(2.0);
+        ses::gpu::Field3D f{g};
+        f.data() = manual;
+        sim.set_psi(f);
+        EXPECT(sim.psi().data() == manual, "set_psi replaces the field");
+        sim.relax(50, 0.01);  // imaginary time keeps the field normalised
+        EXPECT(std::fabs(ses::gpu::norm_sq(sim.psi()) - 1.0) < 1e-12, "relax renormalises");
+    }
     std::printf("%s (%d failures)\n", failures ? "FAILED" : "OK", failures);
     return failures ? 1 : 0;
 }

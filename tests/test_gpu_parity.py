@@ -97,7 +97,7 @@ def test_fft_rejects_unsupported_length(ses):
     with pytest.raises(ValueError):
         ses.fft(np.ones(7, complex))
     with pytest.raises(ValueError):
-        ses.fft(np.ones(8192, complex))  # beyond the 4096 line limit
+        ses.fft(np.ones(7 * 1024, complex))  # above 4096 and not N1 x N2 with compiled factors
 
 
 # ---------------------------------------------------------------- tables

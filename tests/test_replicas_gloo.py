@@ -23,7 +23,7 @@ def worker(rank, world, port, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     specs = scenes.config_c4_specs(256)
-    mine = replicas.route(specs, rank, world)
+    mine = replicas.route_balanced(specs, rank, world, lambda s: s["n"] ** 3)
     pts = sum(s["n"] ** 3 for s in mine)
     total = replicas.sum_over_ranks(pts, dist)
     slowest = replicas.max_over_ranks(10.0 + rank, dist)
@@ -49,6 +49,10 @@ def test_two_gloo_ranks_route_and_reduce():
     assert set(i0).isdisjoint(i1) and sorted(i0 + i1) == list(range(256))
     assert t0 == t1 == sum(s["n"] ** 3 for s in scenes.config_c4_specs(256))
     assert m0 == m1 == 11.0
+    # the balanced split gives each rank the same grid points to within one instance
+    byidx = {s["index"]: s["n"] ** 3 for s in scenes.config_c4_specs(256)}
+    p0, p1 = sum(byidx[i] for i in i0), sum(byidx[i] for i in i1)
+    assert abs(p0 - p1) <= 160 ** 3
     assert sorted(q0 + q1) == list(range(48)) and set(q0).isdisjoint(q1)
 
 
