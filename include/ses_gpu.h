@@ -152,6 +152,13 @@ SES_API ses_status ses_gpu_dt(ses_handle h, double* dt);
  * mean_momentum of the resident psi (observables.ixx:121-234), with xlo/xhi
  * the x-interval of p_range.  Blocks until the values are on the host. */
 SES_API ses_status ses_gpu_observe(ses_handle h, double xlo, double xhi, ses_observables* out);
+/* The same observables queued on the handle's stream (its batch's stream while
+ * it is a member) without waiting, like Engine::step_async / wait_async
+ * (solver/src/vk_engine.ixx:638-698): out receives them once the stream has
+ * reached this point (ses_gpu_sync, ses_batch_sync, or an event the caller
+ * records on that stream).  out should be page-locked host memory; the values
+ * equal ses_gpu_observe's bit for bit. */
+SES_API ses_status ses_gpu_observe_async(ses_handle h, double xlo, double xhi, ses_observables* out);
 /* Engine::readback / upload_state (vk_engine.ixx:2136-2155, 1083-1089,
  * 2413-2421): interleaved complex128 host arrays of N elements (the C64 path
  * rounds on upload and widens on readback).  Both block until done. */

@@ -32,7 +32,7 @@ EXPORTS = [
     "ses_serve_wait_idle", "ses_serve_stats", "ses_serve_close", "ses_gpu_create_imag", "ses_gpu_relax",
     "ses_gpu_step_driven", "ses_gpu_snapshot", "ses_gpu_restore", "ses_gpu_density_slice",
     "ses_batch_observe_some", "ses_batch_run", "ses_gpu_norm_and_peak", "ses_gpu_scale", "ses_gpu_prepare",
-    "ses_batch_prepare", "ses_gpu_set_wait_limit",
+    "ses_batch_prepare", "ses_gpu_set_wait_limit", "ses_gpu_observe_async",
 ]
 
 
@@ -130,6 +130,7 @@ def _load() -> C.CDLL:
         "ses_gpu_prepare": ([hp, C.c_int], st),
         "ses_batch_prepare": ([vp, C.c_int], st),
         "ses_gpu_set_wait_limit": ([hp, C.c_int64, C.c_uint32], st),
+        "ses_gpu_observe_async": ([hp, C.c_double, C.c_double, C.POINTER(Observables)], st),
         "ses_fft3_host": ([C.POINTER(C.c_int32), C.c_int, dp, C.c_int], st),
         "ses_gpu_profile_step": ([hp, C.c_int, C.c_int, dp], st),
         "ses_gpu_autotune": ([hp, C.c_int], st),

@@ -274,6 +274,7 @@ struct ses_solver {
     void* kfull = nullptr;   // kinetic delta per stored k-space element
     void* tw4 = nullptr;     // W_N^{n1 k2} per element (complex64: hi part)
     void* tw4l = nullptr;    // complex64: lo part
+    ses_observables* dobs = nullptr;  // ses_gpu_observe_async: observables finished on the device
 };
 
 namespace {
@@ -304,7 +305,8 @@ void release(ses_solver* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
-    void* ptrs[] = {h->psi, h->scratch, h->vtab, h->V, h->maskfull, h->partials, h->dsums, h->kfull, h->tw4, h->tw4l};
+    void* ptrs[] = {h->psi, h->scratch, h->vtab, h->V, h->maskfull, h->partials, h->dsums, h->kfull, h->tw4, h->tw4l,
+                    h->dobs};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int a = 0; a < 3; ++a) {
@@ -1477,6 +1479,29 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
 }
 
 // Observables from the sums enqueue_observe copied to the host (after a wait).
+// finish_observe on the device, for ses_gpu_observe_async: the same operations
+// in the same order, with round-to-nearest intrinsics so that no multiply-add is
+// contracted (the values equal the host's bit for bit).
+__global__ void finish_observe_kernel(const double* __restrict__ sums, double dv, ses_observables* out) {
+    if (threadIdx.x != 0) return;
+    const double* r = sums;
+    const double* k = sums + kRedR;
+    auto ratio = [](double num, double den) { return den > 0.0 ? __ddiv_rn(num, den) : 0.0; };
+    ses_observables o;
+    o.norm = __dmul_rn(r[0], dv);
+    o.energy_v = ratio(r[1], r[0]);
+    o.energy_t = ratio(k[1], k[0]);
+    o.energy = __dadd_rn(o.energy_v, o.energy_t);
+    o.p_range = __dmul_rn(r[2], dv);
+    for (int a = 0; a < 3; ++a) {
+        o.mean_pos[a] = ratio(r[3 + a], r[0]);
+        const double var = __dsub_rn(ratio(r[6 + a], r[0]), __dmul_rn(o.mean_pos[a], o.mean_pos[a]));
+        o.sigma_pos[a] = __dsqrt_rn(fmax(0.0, var));
+        o.mean_mom[a] = ratio(k[2 + a], k[0]);
+    }
+    *out = o;
+}
+
 void finish_observe(const ses_solver* h, ses_observables* out) {
     const double* r = h->hsums;
     const double* k = h->hsums + kRedR;
@@ -1570,6 +1595,13 @@ struct BatchClass {
     cudaEvent_t done = nullptr;
     cudaGraphExec_t body[2] = {nullptr, nullptr};
     bool dirty = true;
+    // pinned staging of the argument / tensor-map uploads, two buffers used in
+    // turn; staged[i] is recorded after the copies out of hstage[i], so a buffer
+    // is rewritten only once the copy that read it has run
+    unsigned char* hstage[2] = {nullptr, nullptr};
+    size_t hcap[2] = {0, 0};
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    int stage_i = 0;
 };
 
 }  // namespace
@@ -1584,16 +1616,68 @@ struct ses_batch_s {
     std::vector<BatchClass*> classes;
     std::map<std::string, int> sel;    // autotuned variant per class pass (batch_tune_key)
     int sms = 148;
+    // graphs replaced while launches of them may still be queued: destroyed once
+    // the event recorded on the batch stream at their replacement has completed
+    std::vector<std::pair<cudaEvent_t, cudaGraphExec_t>> retired;
 };
 
 namespace {
 
-void drop_class(BatchClass* c) {
+// Host wait (polling, bounded) for an event; false on timeout or device error.
+bool event_wait(cudaEvent_t e, int timeout_ms) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(e);
+        if (q == cudaSuccess) return true;
+        if (q != cudaErrorNotReady) return false;
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms)) return false;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+// A class graph that queued launches may still use: destroyed later (reap).
+void retire_graph(ses_batch_s* b, cudaGraphExec_t g) {
+    if (!g) return;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(e, b->stream) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamSynchronize(b->stream);  // cannot order it: wait, then destroy now
+        if (e) cudaEventDestroy(e);
+        cudaGraphExecDestroy(g);
+        return;
+    }
+    b->retired.emplace_back(e, g);
+}
+
+// Destroy the retired graphs whose launches have all completed (all: the batch is idle).
+void reap(ses_batch_s* b, bool all) {
+    for (size_t i = 0; i < b->retired.size();) {
+        auto& r = b->retired[i];
+        if (all || cudaEventQuery(r.first) == cudaSuccess) {
+            cudaGraphExecDestroy(r.second);
+            cudaEventDestroy(r.first);
+            b->retired.erase(b->retired.begin() + (long)i);
+        } else {
+            ++i;
+        }
+    }
+    cudaGetLastError();  // a not-ready query leaves no error to report
+}
+
+void drop_class(ses_batch_s* b, BatchClass* c) {
     for (auto& g : c->body) {
-        if (g) cudaGraphExecDestroy(g);
+        retire_graph(b, g);
         g = nullptr;
     }
-    if (c->dargs) cudaFree(c->dargs);
+    for (int i = 0; i < 2; ++i) {
+        if (c->staged[i]) {
+            event_wait(c->staged[i], 60000);
+            cudaEventDestroy(c->staged[i]);
+        }
+        if (c->hstage[i]) cudaFreeHost(c->hstage[i]);
+    }
+    if (c->dargs) cudaFree(c->dargs);  // waits for the device: no queued launch reads them any more
     if (c->dmaps) cudaFree(c->dmaps);
     if (c->done) cudaEventDestroy(c->done);
     if (c->cap) cudaStreamDestroy(c->cap);
@@ -1609,6 +1693,7 @@ ses_status batch_wait(ses_batch_s* b, int timeout_ms) {
     for (;;) {
         const cudaError_t q = cudaEventQuery(b->ev);
         if (q == cudaSuccess) {
+            reap(b, false);
             if (*b->herr) {
                 *b->herr = 0;
                 cudaMemsetAsync(b->derr, 0, sizeof(unsigned), b->stream);
@@ -1793,20 +1878,58 @@ ses_status class_upload(const ses_batch_s* b, BatchClass& c) {
                 share_tables(c, i, a);
             }
     class_select<T>(b, c);
-    SES_TRY(class_maps(c, 0, c.dmaps, c.mcap));
-    const size_t bytes = host.size() * sizeof(PassArgs<T>);
-    if (bytes > c.dcap) {
-        if (c.dargs) cudaFree(c.dargs);
-        c.dargs = nullptr;
-        c.dcap = 0;
-        const cudaError_t e = cudaMalloc(&c.dargs, bytes);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return fail(SES_ENOMEM, "batch argument table allocation failed");
-        }
-        c.dcap = bytes;
+    // tensor maps [q][member] of the members' psi for the selected strided variants
+    std::vector<CUtensorMap> maps;
+    bool any = false;
+    for (int q = 0; q < c.nmid; ++q) any = any || c.svar[q] >= 0;
+    if (any) {
+        maps.resize((size_t)3 * nm);
+        for (int q = 0; q < c.nmid; ++q)
+            if (c.svar[q] >= 0)
+                for (size_t i = 0; i < nm; ++i) maps[(size_t)q * nm + i] = c.mem[i]->tmap[0][c.mid_axis[q]][c.svar[q]];
     }
-    SES_CU(cudaMemcpy(c.dargs, host.data(), bytes, cudaMemcpyHostToDevice));
+    const size_t bytes = host.size() * sizeof(PassArgs<T>);
+    const size_t mb = maps.size() * sizeof(CUtensorMap);
+    // device tables grow with headroom; a reallocation waits for the device (cudaFree)
+    auto grow = [&](void** d, size_t& cap, size_t need, const char* what) -> ses_status {
+        if (need <= cap) return SES_OK;
+        if (*d) cudaFree(*d);
+        *d = nullptr;
+        cap = 0;
+        const size_t want = need + need / 2;
+        if (cudaMalloc(d, want) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SES_ENOMEM, std::string("batch ") + what + " table allocation failed");
+        }
+        cap = want;
+        return SES_OK;
+    };
+    SES_TRY(grow(&c.dargs, c.dcap, bytes, "argument"));
+    if (mb) SES_TRY(grow(reinterpret_cast<void**>(&c.dmaps), c.mcap, mb, "tensor map"));
+    // stage in pinned memory and copy in stream order: the copies run after every
+    // launch queued so far on the batch stream (they read the old contents), so
+    // no host wait is needed; the staging buffer is reused two uploads later
+    const int si = c.stage_i;
+    c.stage_i ^= 1;
+    if (!c.staged[si]) SES_CU(cudaEventCreateWithFlags(&c.staged[si], cudaEventDisableTiming));
+    else if (!event_wait(c.staged[si], 600000)) return fail(SES_ETIMEDOUT, "batch argument staging wait expired");
+    const size_t sb = bytes + ((mb + 63) / 64) * 64 + 64;
+    if (sb > c.hcap[si]) {
+        if (c.hstage[si]) cudaFreeHost(c.hstage[si]);
+        c.hstage[si] = nullptr;
+        c.hcap[si] = 0;
+        if (cudaMallocHost(reinterpret_cast<void**>(&c.hstage[si]), sb + sb / 2) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SES_ENOMEM, "pinned staging allocation failed");
+        }
+        c.hcap[si] = sb + sb / 2;
+    }
+    const size_t moff = ((bytes + 63) / 64) * 64;
+    std::memcpy(c.hstage[si], host.data(), bytes);
+    if (mb) std::memcpy(c.hstage[si] + moff, maps.data(), mb);
+    SES_CU(cudaMemcpyAsync(c.dargs, c.hstage[si], bytes, cudaMemcpyHostToDevice, b->stream));
+    if (mb) SES_CU(cudaMemcpyAsync(c.dmaps, c.hstage[si] + moff, mb, cudaMemcpyHostToDevice, b->stream));
+    SES_CU(cudaEventRecord(c.staged[si], b->stream));
     return SES_OK;
 }
 
@@ -1955,11 +2078,13 @@ ses_status batch_refresh(ses_batch_s* b) {
     bool any_dirty = false;
     for (BatchClass* c : b->classes) any_dirty |= c->dirty;
     if (!any_dirty) return SES_OK;
-    SES_TRY(batch_wait(b, 0));  // no launch in flight reads the tables being replaced
+    // the new tables are uploaded in stream order (class_upload); launches queued
+    // before read the old ones, so nothing waits here
+    reap(b, false);
     for (BatchClass* c : b->classes) {
         if (!c->dirty || c->mem.empty()) continue;
         for (auto& g : c->body) {
-            if (g) cudaGraphExecDestroy(g);
+            retire_graph(b, g);
             g = nullptr;
         }
         SES_TRY(c->prec == SES_C128 ? class_upload<double>(b, *c) : class_upload<float>(b, *c));
@@ -2068,7 +2193,10 @@ ses_status class_autotune(ses_batch_s* b, BatchClass& c, std::map<std::string, i
 ses_status batch_remove_impl(ses_batch_s* b, ses_solver* h) {
     auto it = std::find(b->members.begin(), b->members.end(), h);
     if (it == b->members.end()) return fail(SES_ENOTFOUND, "handle is not a member of this batch");
-    SES_TRY(batch_wait(b, 0));
+    // the handle's own stream waits for everything queued on the batch so far
+    // (its steps included): no host wait
+    SES_CU(cudaEventRecord(h->ev, b->stream));
+    SES_CU(cudaStreamWaitEvent(h->own, h->ev, 0));
     b->members.erase(it);
     BatchClass* c = find_class(b, h);
     if (c) {
@@ -2076,7 +2204,7 @@ ses_status batch_remove_impl(ses_batch_s* b, ses_solver* h) {
         c->dirty = true;
         if (c->mem.empty()) {
             b->classes.erase(std::find(b->classes.begin(), b->classes.end(), c));
-            drop_class(c);
+            drop_class(b, c);
         }
     }
     h->batch = nullptr;
@@ -2343,6 +2471,19 @@ ses_status ses_gpu_observe(ses_handle h, double xlo, double xhi, ses_observables
     return SES_OK;
 }
 
+ses_status ses_gpu_observe_async(ses_handle h, double xlo, double xhi, ses_observables* out) {
+    SES_TRY(check_handle(h));
+    if (!out) return fail(SES_EINVAL, "null output");
+    if (!h->dobs) SES_TRY(dalloc(h, reinterpret_cast<void**>(&h->dobs), sizeof(ses_observables)));
+    SES_TRY(h->prec == SES_C128 ? enqueue_observe<double>(h, xlo, xhi) : enqueue_observe<float>(h, xlo, xhi));
+    const double dv = ((h->box[1] - h->box[0]) / phys_n(h, 0)) * ((h->box[3] - h->box[2]) / phys_n(h, 1)) *
+                      ((h->box[5] - h->box[4]) / phys_n(h, 2));
+    finish_observe_kernel<<<1, 32, 0, h->stream>>>(h->dsums, dv, h->dobs);
+    SES_CU(cudaGetLastError());
+    SES_CU(cudaMemcpyAsync(out, h->dobs, sizeof(ses_observables), cudaMemcpyDeviceToHost, h->stream));
+    return SES_OK;
+}
+
 ses_status ses_gpu_write_psi(ses_handle h, const double* psi_in) {
     SES_TRY(check_handle(h));
     if (!psi_in) return fail(SES_EINVAL, "null psi");
@@ -2594,7 +2735,9 @@ ses_status ses_batch_destroy(ses_batch b) {
         h->batch = nullptr;
         h->stream = h->own;
     }
-    for (BatchClass* c : b->classes) drop_class(c);
+    for (BatchClass* c : b->classes) drop_class(b, c);
+    cudaStreamSynchronize(b->stream);
+    reap(b, true);
     if (b->derr) cudaFree(b->derr);
     if (b->herr) cudaFreeHost(b->herr);
     if (b->ev) cudaEventDestroy(b->ev);
@@ -2610,7 +2753,9 @@ ses_status ses_batch_add(ses_batch b, ses_handle h) {
     if (h->batch) return fail(SES_EBUSY, "handle already belongs to a batch");
     if (!h->with_tables) return fail(SES_EINVAL, "handle has no phase tables");
     if (h->dev != b->dev) return fail(SES_EINVAL, "handle and batch are on different devices");
-    SES_TRY(wait_bounded(h, 0));
+    // the batch stream waits for the handle's queued work (uploads, table builds): no host wait
+    SES_CU(cudaEventRecord(h->ev, h->stream));
+    SES_CU(cudaStreamWaitEvent(b->stream, h->ev, 0));
     h->batch = b;
     h->stream = b->stream;
     b->members.push_back(h);

@@ -7,10 +7,12 @@
 // a member of one ses_batch, and advances all members together in rounds.  A
 // round ends at the earliest observation point or completion of any member,
 // so new requests join (and finished ones leave) between rounds while the
-// others keep stepping.  Observations stream back as records; latency is
-// submission to completion.
+// others keep stepping; two rounds are kept queued so that the device never
+// waits for the host's bookkeeping.  Observations stream back as records;
+// latency is submission to completion.
 //
-// Built only on the public C ABI (ses_gpu_*, ses_batch_*): one worker thread
+// Built on the public C ABI (ses_gpu_*, ses_batch_*) plus one CUDA stream and
+// events of its own (the batch's stream, round boundaries): one worker thread
 // owns the batch and every handle; callers only touch the queues under a mutex.
 #include <cuda_runtime_api.h>
 
@@ -100,6 +102,11 @@ struct ses_server_s {
     // worker-owned
     std::vector<std::shared_ptr<Request>> active;
     size_t used = 0;
+    cudaStream_t stream = nullptr;              // the batch's stream: rounds, joins, observations
+    cudaEvent_t ev_start[2] = {nullptr, nullptr};  // per round parity: start and end of a queued round
+    cudaEvent_t ev_end[2] = {nullptr, nullptr};
+    ses_observables* obuf[2] = {nullptr, nullptr};  // pinned observable slots per round parity
+    size_t ocap[2] = {0, 0};
 
     // statistics (under mu)
     int64_t submitted = 0, admitted = 0, completed = 0, cancelled = 0, failed = 0, rounds = 0;
@@ -116,17 +123,6 @@ int next_event(const Request& r) {
     int e = r.nsteps;
     if (r.every > 0) e = std::min(e, (r.done / r.every + 1) * r.every);
     return e;
-}
-
-void push_record(ses_server_s* s, Request& r, const ses_observables& o, bool fin) {
-    ses_record rec{};
-    rec.id = r.id;
-    rec.step = r.done;
-    rec.final_record = fin ? 1 : 0;
-    rec.t_ms = ms_since(r.t_submit);
-    rec.obs = o;
-    std::lock_guard<std::mutex> lk(s->mu);
-    r.records.push_back(rec);
 }
 
 // Publish a request's final state (worker thread); its handle is released by the caller.
@@ -195,40 +191,192 @@ int create_one(ses_server_s* s, const std::shared_ptr<Request>& r, bool others_h
     return 0;
 }
 
-// The worker: rounds run asynchronously on the batch stream while the host
-// admits new requests (creates their handles and tables) and reads back the
-// fields of requests that finished in the previous round; handles are freed
-// only between rounds (freeing device memory waits for the device).
+// One queued round: every member advances R merged Strang steps; the listed
+// observers are observed at its end (asynchronously, into pinned slots) and the
+// finishers leave the batch there.
+struct Round {
+    int R = 0;
+    int slot = 0;  // pinned observable buffer and event pair (round parity)
+    double pts = 0;
+    std::vector<std::shared_ptr<Request>> observers;
+    std::vector<int> obs_step;
+    std::vector<std::shared_ptr<Request>> finishers;
+};
+
+// The worker keeps up to two rounds queued on the server's stream, so the
+// device steps round k+1 while the host publishes round k, admits new requests
+// (creates their handles and tables) and reads back finished fields.  Joining,
+// leaving, stepping and observing are all stream-ordered (no host wait); the host
+// waits only for the oldest round's end event.  A round ends at the earliest
+// observation point or completion of any member.
 void worker_main(ses_server_s* s) {
     cudaSetDevice(s->dev);
-    std::vector<std::shared_ptr<Request>> pending;    // created, join the batch before the next round
-    std::vector<std::shared_ptr<Request>> finishing;  // left the batch, field still to read back
-    std::vector<std::shared_ptr<Request>> zombies;    // read back, handle to free between rounds
-    bool inflight = false;
-    int R = 0;
-    Clock::time_point t_round;
-    auto fail_active = [&](const std::string& err) {
+    std::deque<Round> q;
+    std::vector<std::shared_ptr<Request>> pending;  // created, join the batch at the next planned round
+    long long round_no = 0;
+    auto fail_everything = [&](const std::string& err) {
         for (const auto& r : s->active) retire(s, r, SES_REQ_FAILED, err);
         s->active.clear();
+        for (Round& rd : q)
+            for (const auto& r : rd.finishers) retire(s, r, SES_REQ_FAILED, err);
+        q.clear();
+    };
+    auto cancelled = [&](const std::shared_ptr<Request>& r) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        return r->cancel;
     };
     for (;;) {
-        // 1. admission, first come first served while the estimate fits the budget
-        //    (overlaps the round in flight)
+        // A. the oldest queued round: wait for its end, publish its observations and results
+        if (!q.empty()) {
+            Round rd = std::move(q.front());
+            q.pop_front();
+            const cudaEvent_t e1 = s->ev_end[rd.slot];
+            const auto t0 = Clock::now();
+            cudaError_t qe;
+            while ((qe = cudaEventQuery(e1)) == cudaErrorNotReady) {
+                if (ms_since(t0) > 600000.0) break;
+                std::this_thread::sleep_for(std::chrono::microseconds(20));
+            }
+            int derr = 0;
+            ses_status st = qe == cudaSuccess ? SES_OK : (qe == cudaErrorNotReady ? SES_ETIMEDOUT : SES_EDEVICE);
+            // the batch's error word (an expired bounded wait in a pipelined pass) is
+            // read when nothing else is queued, so the check never drains the queue
+            if (st == SES_OK && q.empty()) st = ses_batch_sync(s->batch, 600000);
+            if (st != SES_OK) {
+                derr = 1;
+                const std::string err = qe == cudaSuccess ? ses_last_error() : "round did not complete";
+                for (const auto& r : rd.finishers) retire(s, r, SES_REQ_FAILED, err);
+                fail_everything(err);
+                cudaGetLastError();
+            }
+            if (!derr) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, s->ev_start[rd.slot], e1);
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    ++s->rounds;
+                    s->gridpt_steps += rd.pts;
+                    s->busy_ms += ms;
+                }
+                const ses_observables* ob = s->obuf[rd.slot];
+                for (size_t j = 0; j < rd.observers.size(); ++j) {
+                    Request& r = *rd.observers[j];
+                    const int step = rd.obs_step[j];
+                    ses_record rec{};
+                    rec.id = r.id;
+                    rec.step = step;
+                    rec.final_record = step >= r.nsteps ? 1 : 0;
+                    rec.t_ms = ms_since(r.t_submit);
+                    rec.obs = ob[j];
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    r.records.push_back(rec);
+                }
+                for (const auto& r : rd.finishers) {  // off the batch since this round's end
+                    std::vector<double> out((size_t)grid_points(r->grid) * 2);
+                    const ses_status rs = ses_gpu_read_psi(r->h, out.data());
+                    const std::string err = rs == SES_OK ? "" : ses_last_error();
+                    {
+                        std::lock_guard<std::mutex> lk(s->mu);
+                        r->result.swap(out);
+                        r->result_ready = rs == SES_OK;
+                    }
+                    retire(s, r, rs == SES_OK ? SES_REQ_DONE : SES_REQ_FAILED, err);
+                }
+            }
+        }
+
+        // B. cancellations of running requests: they leave the batch (stream-ordered) and are freed
+        for (size_t i = 0; i < s->active.size();) {
+            if (cancelled(s->active[i])) {
+                ses_batch_remove(s->batch, s->active[i]->h);
+                retire(s, s->active[i], SES_REQ_CANCELLED, "");
+                s->active.erase(s->active.begin() + (long)i);
+            } else {
+                ++i;
+            }
+        }
+
+        // C. plan and queue rounds until two are in flight
+        while (q.size() < 2) {
+            for (const auto& r : pending) {
+                if (cancelled(r)) {
+                    retire(s, r, SES_REQ_CANCELLED, "");
+                    continue;
+                }
+                const ses_status st = ses_batch_add(s->batch, r->h);
+                if (st != SES_OK) {
+                    retire(s, r, SES_REQ_FAILED, ses_last_error());
+                    continue;
+                }
+                s->active.push_back(r);
+            }
+            pending.clear();
+            if (s->active.empty()) break;
+            Round rd;
+            rd.slot = (int)(round_no & 1);
+            rd.R = s->max_round;
+            for (const auto& r : s->active) rd.R = std::min(rd.R, next_event(*r) - r->done);
+            rd.R = std::max(rd.R, 1);
+            cudaEventRecord(s->ev_start[rd.slot], s->stream);
+            ses_status st = ses_batch_step(s->batch, rd.R, 1);
+            for (const auto& r : s->active) {
+                r->done += rd.R;
+                rd.pts += (double)grid_points(r->grid) * rd.R;
+                if (r->done >= r->nsteps || (r->every > 0 && r->done % r->every == 0)) {
+                    rd.observers.push_back(r);
+                    rd.obs_step.push_back(r->done);
+                }
+            }
+            if (st == SES_OK && rd.observers.size() > s->ocap[rd.slot]) {
+                if (s->obuf[rd.slot]) cudaFreeHost(s->obuf[rd.slot]);
+                s->obuf[rd.slot] = nullptr;
+                s->ocap[rd.slot] = 0;
+                const size_t want = rd.observers.size() * 2 + 16;
+                if (cudaMallocHost(reinterpret_cast<void**>(&s->obuf[rd.slot]), want * sizeof(ses_observables)) ==
+                    cudaSuccess)
+                    s->ocap[rd.slot] = want;
+                else
+                    st = sfail(SES_ENOMEM, "pinned observable buffer allocation failed");
+            }
+            for (size_t j = 0; st == SES_OK && j < rd.observers.size(); ++j) {
+                const Request& r = *rd.observers[j];
+                st = ses_gpu_observe_async(r.h, r.xlo, r.xhi, &s->obuf[rd.slot][j]);
+            }
+            for (size_t i = 0; st == SES_OK && i < s->active.size();) {
+                std::shared_ptr<Request> r = s->active[i];
+                if (r->done >= r->nsteps) {
+                    st = ses_batch_remove(s->batch, r->h);  // its own stream waits for this round
+                    rd.finishers.push_back(r);
+                    s->active.erase(s->active.begin() + (long)i);
+                    continue;
+                }
+                ++i;
+            }
+            if (st == SES_OK && cudaEventRecord(s->ev_end[rd.slot], s->stream) != cudaSuccess)
+                st = sfail(SES_EDEVICE, "event record failed");
+            if (st != SES_OK) {
+                const std::string err = ses_last_error();
+                for (const auto& r : rd.finishers) retire(s, r, SES_REQ_FAILED, err);
+                fail_everything(err);
+                break;
+            }
+            q.push_back(std::move(rd));
+            ++round_no;
+        }
+
+        // D. admission, first come first served while the estimate fits the budget:
+        //    with rounds queued, a few requests per pass (their set-up overlaps the
+        //    device's work); with nothing to run, one, which then starts stepping
         std::vector<std::shared_ptr<Request>> take;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            if (!inflight && s->active.empty() && pending.empty() && finishing.empty() && s->queue.empty()) {
+            if (q.empty() && s->active.empty() && pending.empty() && s->queue.empty()) {
                 s->idle.notify_all();
                 s->cv.wait(lk, [&] { return s->stop || !s->queue.empty(); });
             }
-            if (s->stop && s->queue.empty() && s->active.empty() && pending.empty() && !inflight &&
-                finishing.empty())
-                break;
+            if (s->stop && s->queue.empty() && s->active.empty() && pending.empty() && q.empty()) break;
             size_t room = s->budget > s->used ? s->budget - s->used : 0;
-            // while the device has work, admit a few requests per round (their set-up
-            // overlaps the round); with nothing to run, admit one and start stepping it
-            const bool busy = inflight || !s->active.empty() || !pending.empty();
-            const size_t cap = busy ? (size_t)kAdmitPerRound : 1;
+            const size_t cap = q.empty() ? 1 : (size_t)kAdmitPerRound;
             while (!s->queue.empty() && take.size() < cap) {
                 std::shared_ptr<Request> r = s->queue.front();
                 if (r->cancel) {
@@ -245,7 +393,7 @@ void worker_main(ses_server_s* s) {
             }
         }
         for (size_t i = 0; i < take.size(); ++i) {
-            const bool others = inflight || !s->active.empty() || !pending.empty() || !zombies.empty();
+            const bool others = !q.empty() || !s->active.empty() || !pending.empty();
             const int c = create_one(s, take[i], others);
             if (c == 0) pending.push_back(take[i]);
             if (c == 1) {  // out of device memory: back to the head of the queue
@@ -254,141 +402,11 @@ void worker_main(ses_server_s* s) {
                 break;
             }
         }
-
-        // 2. the round in flight: wait, free what finished before it, observe, collect finished
-        if (inflight) {
-            ses_status st = ses_batch_sync(s->batch, 600000);
-            inflight = false;
-            const double round_ms = ms_since(t_round);
-            for (const auto& r : zombies) release_handle(s, r);
-            zombies.clear();
-            if (st != SES_OK) {
-                fail_active(ses_last_error());
-            } else {
-                double pts = 0;
-                for (const auto& r : s->active) pts += (double)grid_points(r->grid) * R;
-                {
-                    std::lock_guard<std::mutex> lk(s->mu);
-                    ++s->rounds;
-                    s->gridpt_steps += pts;
-                    s->busy_ms += round_ms;
-                }
-                std::vector<ses_handle> oh;
-                std::vector<double> olo, ohi;
-                std::vector<size_t> oi;
-                for (size_t i = 0; i < s->active.size(); ++i) {
-                    Request& r = *s->active[i];
-                    r.done += R;
-                    if (r.done >= r.nsteps || (r.every > 0 && r.done % r.every == 0)) {
-                        oh.push_back(r.h);
-                        olo.push_back(r.xlo);
-                        ohi.push_back(r.xhi);
-                        oi.push_back(i);
-                    }
-                }
-                std::vector<ses_observables> obs(oh.size());
-                if (!oh.empty())
-                    st = ses_batch_observe_some(s->batch, oh.data(), (int)oh.size(), olo.data(), ohi.data(),
-                                                obs.data());
-                if (st != SES_OK) {
-                    fail_active(ses_last_error());
-                } else {
-                    for (size_t q = 0; q < oi.size(); ++q) {
-                        Request& r = *s->active[oi[q]];
-                        push_record(s, r, obs[q], r.done >= r.nsteps);
-                    }
-                    for (size_t i = 0; i < s->active.size();) {
-                        std::shared_ptr<Request> r = s->active[i];
-                        if (r->done >= r->nsteps) {
-                            // leaves the batch: its own stream from now on
-                            if (ses_batch_remove(s->batch, r->h) == SES_OK)
-                                finishing.push_back(r);
-                            else
-                                retire(s, r, SES_REQ_FAILED, ses_last_error());
-                            s->active.erase(s->active.begin() + (long)i);
-                            continue;
-                        }
-                        ++i;
-                    }
-                }
-            }
-        } else {
-            for (const auto& r : zombies) release_handle(s, r);
-            zombies.clear();
-        }
-
-        // 3. cancellations of running requests (no round in flight)
-        for (size_t i = 0; i < s->active.size();) {
-            bool c;
-            {
-                std::lock_guard<std::mutex> lk(s->mu);
-                c = s->active[i]->cancel;
-            }
-            if (c) {
-                retire(s, s->active[i], SES_REQ_CANCELLED, "");
-                s->active.erase(s->active.begin() + (long)i);
-            } else {
-                ++i;
-            }
-        }
-
-        // 4. new members join, then the next round is queued: up to the earliest
-        //    observation point or completion of any member
-        for (const auto& r : pending) {
-            bool c;
-            {
-                std::lock_guard<std::mutex> lk(s->mu);
-                c = r->cancel;
-            }
-            if (c) {
-                retire(s, r, SES_REQ_CANCELLED, "");
-                continue;
-            }
-            const ses_status st = ses_batch_add(s->batch, r->h);
-            if (st != SES_OK) {
-                retire(s, r, SES_REQ_FAILED, ses_last_error());
-                continue;
-            }
-            s->active.push_back(r);
-        }
-        pending.clear();
-        if (!s->active.empty()) {
-            R = s->max_round;
-            for (const auto& r : s->active) R = std::min(R, next_event(*r) - r->done);
-            R = std::max(R, 1);
-            t_round = Clock::now();
-            const ses_status st = ses_batch_step(s->batch, R, 1);
-            if (st != SES_OK)
-                fail_active(ses_last_error());
-            else
-                inflight = true;
-        }
-
-        // 5. results of the requests that finished, read back while the round runs
-        for (const auto& r : finishing) {
-            std::vector<double> out((size_t)grid_points(r->grid) * 2);
-            const ses_status st = ses_gpu_read_psi(r->h, out.data());
-            const std::string err = st == SES_OK ? "" : ses_last_error();
-            {
-                std::lock_guard<std::mutex> lk(s->mu);
-                r->result.swap(out);
-                r->result_ready = st == SES_OK;
-            }
-            // with a round in flight the handle is freed after it (its bytes stay counted until then)
-            if (inflight) {
-                publish(s, r, st == SES_OK ? SES_REQ_DONE : SES_REQ_FAILED, err);
-                zombies.push_back(r);
-            } else {
-                retire(s, r, st == SES_OK ? SES_REQ_DONE : SES_REQ_FAILED, err);
-            }
-        }
-        finishing.clear();
-        if (!inflight && s->active.empty() && pending.empty()) {
+        if (q.empty() && s->active.empty() && pending.empty()) {
             std::lock_guard<std::mutex> lk(s->mu);
             if (s->queue.empty()) s->idle.notify_all();
         }
     }
-    for (const auto& r : zombies) release_handle(s, r);
     std::lock_guard<std::mutex> lk(s->mu);
     s->idle.notify_all();
 }
@@ -415,8 +433,16 @@ ses_status ses_serve_open(size_t budget_bytes, int max_round_steps, ses_server* 
     s->budget = budget_bytes;
     s->max_round = max_round_steps > 0 ? max_round_steps : 100;
     cudaGetDevice(&s->dev);
-    const ses_status st = ses_batch_create(&s->batch);
+    ses_status st = ses_batch_create(&s->batch);
+    if (st == SES_OK && cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        st = sfail(SES_EDEVICE, "stream creation failed");
+    for (int i = 0; st == SES_OK && i < 2; ++i)
+        if (cudaEventCreate(&s->ev_start[i]) != cudaSuccess || cudaEventCreate(&s->ev_end[i]) != cudaSuccess)
+            st = sfail(SES_EDEVICE, "event creation failed");
+    if (st == SES_OK) st = ses_batch_set_stream(s->batch, s->stream);
     if (st != SES_OK) {
+        if (s->batch) ses_batch_destroy(s->batch);
+        if (s->stream) cudaStreamDestroy(s->stream);
         delete s;
         return st;
     }
@@ -560,6 +586,13 @@ ses_status ses_serve_close(ses_server s) {
     for (auto& r : s->active)
         if (r->h) ses_gpu_destroy(r->h);
     ses_batch_destroy(s->batch);
+    cudaStreamSynchronize(s->stream);
+    for (int i = 0; i < 2; ++i) {
+        if (s->ev_start[i]) cudaEventDestroy(s->ev_start[i]);
+        if (s->ev_end[i]) cudaEventDestroy(s->ev_end[i]);
+        if (s->obuf[i]) cudaFreeHost(s->obuf[i]);
+    }
+    cudaStreamDestroy(s->stream);
     delete s;
     return SES_OK;
 }
