@@ -282,16 +282,56 @@ namespace {
 // Physical axis length (the layout axes of a long line differ from it).
 int phys_n(const ses_solver* h, int a) { return h->long1d ? (a == 0 ? (int)h->N : 1) : h->n[a]; }
 
+// Device buffers of a handle come from the stream-ordered allocator on the
+// handle's current stream (every later use of them is ordered after it), and go
+// back to it with cudaFreeAsync: creating and destroying handles while other
+// work runs (serving) never synchronises the device, as cudaMalloc / cudaFree can.
 ses_status dalloc(ses_solver* h, void** p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
-        return fail(SES_ENOMEM, "cudaMalloc(" + std::to_string(bytes) + " B) failed: " +
+        return fail(SES_ENOMEM, "cudaMallocAsync(" + std::to_string(bytes) + " B) failed: " +
                                     cudaGetErrorString(e));
     }
     h->bytes += bytes;
     return SES_OK;
+}
+
+// Small page-locked host buffers (observable sums, error words), carved once from
+// 64 KiB chunks and recycled: unlike cudaFreeHost, returning one needs no device
+// synchronisation.  Slots are 256 bytes; chunks live until the process exits.
+class PinnedSlab {
+  public:
+    static constexpr size_t kSlot = 256, kChunk = 64 * 1024;
+    void* get() {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (free_.empty()) {
+            void* c = nullptr;
+            if (cudaMallocHost(&c, kChunk) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            for (size_t o = 0; o < kChunk; o += kSlot) free_.push_back(static_cast<char*>(c) + o);
+        }
+        void* p = free_.back();
+        free_.pop_back();
+        return p;
+    }
+    void put(void* p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lk(mu_);
+        free_.push_back(p);
+    }
+
+  private:
+    std::mutex mu_;
+    std::vector<void*> free_;
+};
+
+PinnedSlab& pinned_slab() {
+    static PinnedSlab slab;
+    return slab;
 }
 
 void drop_graphs(ses_solver* h) {
@@ -303,25 +343,28 @@ void drop_graphs(ses_solver* h) {
 
 void release(ses_solver* h) {
     if (!h) return;
-    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->stream) cudaStreamSynchronize(h->stream);  // the handle's queued work is done
     drop_graphs(h);
+    // back to the stream-ordered allocator (no device-wide synchronisation)
+    cudaStream_t fs = h->own ? h->own : h->stream;
+    auto dfree = [&](void* p) {
+        if (p) cudaFreeAsync(p, fs);
+    };
     void* ptrs[] = {h->psi, h->scratch, h->vtab, h->V, h->maskfull, h->partials, h->dsums, h->kfull, h->tw4, h->tw4l,
-                    h->dobs};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+                    h->dobs, h->derr};
+    for (void* p : ptrs) dfree(p);
     for (int a = 0; a < 3; ++a) {
-        if (h->tw[a]) cudaFree(h->tw[a]);
-        if (h->kv[a]) cudaFree(h->kv[a]);
-        if (h->kd[a]) cudaFree(h->kd[a]);
-        if (h->mask1[a]) cudaFree(h->mask1[a]);
-        if (h->mask1f[a]) cudaFree(h->mask1f[a]);
-        if (h->kdf[a]) cudaFree(h->kdf[a]);
-        if (h->stw[a]) cudaFree(h->stw[a]);
-        if (h->stwl[a]) cudaFree(h->stwl[a]);
+        dfree(h->tw[a]);
+        dfree(h->kv[a]);
+        dfree(h->kd[a]);
+        dfree(h->mask1[a]);
+        dfree(h->mask1f[a]);
+        dfree(h->kdf[a]);
+        dfree(h->stw[a]);
+        dfree(h->stwl[a]);
     }
-    if (h->hsums) cudaFreeHost(h->hsums);
-    if (h->herr) cudaFreeHost(h->herr);
-    if (h->derr) cudaFree(h->derr);
+    pinned_slab().put(h->hsums);
+    pinned_slab().put(h->herr);
     if (h->ev) cudaEventDestroy(h->ev);
     if (h->cap) cudaStreamDestroy(h->cap);
     if (h->own) cudaStreamDestroy(h->own);
@@ -999,12 +1042,31 @@ std::string tune_key(const ses_solver* h, int axis) {
     return k.str();
 }
 
+// The cache file's entries, re-read only when its path, size or modification time
+// changes (batches look them up at every membership change).
 std::map<std::string, int> read_tune_cache() {
+    static std::mutex mu;
+    static std::string last_path;
+    static long long last_mtime = -1, last_size = -1;
+    static std::map<std::string, int> last;
+    const std::string path = tune_cache_path();
+    struct stat st{};
+    const bool exists = stat(path.c_str(), &st) == 0;
+    const long long mtime = exists ? (long long)st.st_mtim.tv_sec * 1000000000LL + st.st_mtim.tv_nsec : -1;
+    const long long size = exists ? (long long)st.st_size : -1;
+    std::lock_guard<std::mutex> lk(mu);
+    if (path == last_path && mtime == last_mtime && size == last_size) return last;
     std::map<std::string, int> m;
-    std::ifstream f(tune_cache_path());
-    std::string key;
-    int v;
-    while (f >> key >> v) m[key] = v;
+    if (exists) {
+        std::ifstream f(path);
+        std::string key;
+        int v;
+        while (f >> key >> v) m[key] = v;
+    }
+    last_path = path;
+    last_mtime = mtime;
+    last_size = size;
+    last = m;
     return m;
 }
 
@@ -1225,7 +1287,7 @@ ses_status upload_stage_twiddles(ses_solver* h) {
         const size_t cnt = t.size() / 2;
         if (h->prec == SES_C128) {
             SES_TRY(dalloc(h, &h->stw[a], cnt * sizeof(cx<double>)));
-            SES_CU(cudaMemcpy(h->stw[a], t.data(), cnt * sizeof(cx<double>), cudaMemcpyHostToDevice));
+            SES_CU(cudaMemcpyAsync(h->stw[a], t.data(), cnt * sizeof(cx<double>), cudaMemcpyHostToDevice, h->stream));
         } else {
             std::vector<float> hi(2 * cnt), lo(2 * cnt);
             for (size_t i = 0; i < 2 * cnt; ++i) {
@@ -1234,8 +1296,8 @@ ses_status upload_stage_twiddles(ses_solver* h) {
             }
             SES_TRY(dalloc(h, &h->stw[a], cnt * sizeof(cx<float>)));
             SES_TRY(dalloc(h, &h->stwl[a], cnt * sizeof(cx<float>)));
-            SES_CU(cudaMemcpy(h->stw[a], hi.data(), cnt * sizeof(cx<float>), cudaMemcpyHostToDevice));
-            SES_CU(cudaMemcpy(h->stwl[a], lo.data(), cnt * sizeof(cx<float>), cudaMemcpyHostToDevice));
+            SES_CU(cudaMemcpyAsync(h->stw[a], hi.data(), cnt * sizeof(cx<float>), cudaMemcpyHostToDevice, h->stream));
+            SES_CU(cudaMemcpyAsync(h->stwl[a], lo.data(), cnt * sizeof(cx<float>), cudaMemcpyHostToDevice, h->stream));
         }
     }
     return SES_OK;
@@ -1405,10 +1467,9 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
     h->partial_rows = rows;
     if ((st = dalloc(h, (void**)&h->partials, rows * kRedR * sizeof(double))) != SES_OK) return bail(st);
     if ((st = dalloc(h, (void**)&h->dsums, 32 * sizeof(double))) != SES_OK) return bail(st);
-    if (cudaMallocHost((void**)&h->hsums, 32 * sizeof(double)) != cudaSuccess) {
-        cudaGetLastError();
+    static_assert(32 * sizeof(double) <= PinnedSlab::kSlot, "observable sums fit a pinned slot");
+    if (!(h->hsums = static_cast<double*>(pinned_slab().get())))
         return bail(fail(SES_ENOMEM, "pinned host allocation failed"));
-    }
     for (int a = 0; a < 3; ++a) {
         // wavenumber / kinetic tables follow the physical axis (a long line's x
         // tables cover the whole line); FFT twiddles follow the layout axis
@@ -1446,10 +1507,8 @@ ses_status create_impl(const ses_grid_desc* grid, ses_precision prec, double dt,
     if (cudaGetLastError() != cudaSuccess) return bail(fail(SES_EDEVICE, "axis table build failed"));
     if ((st = upload_stage_twiddles(h)) != SES_OK) return bail(st);
     if ((st = dalloc(h, (void**)&h->derr, sizeof(unsigned))) != SES_OK) return bail(st);
-    if (cudaMallocHost((void**)&h->herr, sizeof(unsigned)) != cudaSuccess) {
-        cudaGetLastError();
+    if (!(h->herr = static_cast<unsigned*>(pinned_slab().get())))
         return bail(fail(SES_ENOMEM, "pinned host allocation failed"));
-    }
     *h->herr = 0;
     if (cudaMemsetAsync(h->derr, 0, sizeof(unsigned), h->stream) != cudaSuccess)
         return bail(fail(SES_EDEVICE, "memset failed"));
@@ -2341,9 +2400,9 @@ ses_status ses_gpu_set_absorber_separable(ses_handle h, const double* mx, const 
     for (int a = 0; a < 3; ++a) {
         if (!h->mask1[a]) SES_TRY(dalloc(h, (void**)&h->mask1[a], (size_t)h->n[a] * sizeof(double)));
         if (!h->mask1f[a]) SES_TRY(dalloc(h, (void**)&h->mask1f[a], (size_t)h->n[a] * sizeof(float)));
-        SES_CU(cudaMemcpy(h->mask1[a], m[a], (size_t)h->n[a] * sizeof(double), cudaMemcpyHostToDevice));
+        SES_CU(cudaMemcpyAsync(h->mask1[a], m[a], (size_t)h->n[a] * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         std::vector<float> mf(m[a], m[a] + h->n[a]);
-        SES_CU(cudaMemcpy(h->mask1f[a], mf.data(), (size_t)h->n[a] * sizeof(float), cudaMemcpyHostToDevice));
+        SES_CU(cudaMemcpyAsync(h->mask1f[a], mf.data(), (size_t)h->n[a] * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     }
     h->has_mask = true;
     return SES_OK;
@@ -2387,7 +2446,7 @@ ses_status ses_gpu_set_absorber(ses_handle h, const double* mask) {
         h->mask1f[a] = nullptr;
     }
     if (!h->maskfull) SES_TRY(dalloc(h, (void**)&h->maskfull, h->N * sizeof(double)));
-    SES_CU(cudaMemcpy(h->maskfull, mask, h->N * sizeof(double), cudaMemcpyHostToDevice));
+    SES_CU(cudaMemcpyAsync(h->maskfull, mask, h->N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     h->has_mask = true;
     return SES_OK;
 }

@@ -7,8 +7,8 @@
 // a member of one ses_batch, and advances all members together in rounds.  A
 // round ends at the earliest observation point or completion of any member,
 // so new requests join (and finished ones leave) between rounds while the
-// others keep stepping; two rounds are kept queued so that the device never
-// waits for the host's bookkeeping.  Observations stream back as records;
+// others keep stepping; rounds are queued ahead so that the device never waits
+// for the host's bookkeeping.  Observations stream back as records;
 // latency is submission to completion.
 //
 // Built on the public C ABI (ses_gpu_*, ses_batch_*) plus one CUDA stream and
@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -37,9 +38,6 @@ void set_last_error(const std::string& msg);  // ses_gpu.cu
 namespace {
 
 using Clock = std::chrono::steady_clock;
-
-// Requests admitted (handles created) per round while other requests run.
-constexpr int kAdmitPerRound = 4;
 
 ses_status sfail(ses_status s, const std::string& msg) {
     sesk::set_last_error(msg);
@@ -80,6 +78,8 @@ struct Request {
     ses_handle h = nullptr;
     size_t bytes = 0;
     int done = 0;
+    int final_state = SES_REQ_DONE;  // what the finisher publishes
+    std::string final_err;
 };
 
 }  // namespace
@@ -88,30 +88,36 @@ struct ses_server_s {
     int dev = 0;
     size_t budget = 0;
     int max_round = 100;
+    // SES_SERVE_ALIGN=1: requests join only on a grid of max_round steps of the
+    // server's clock, so that members observing every max_round steps observe at
+    // the same round ends (fewer, longer rounds; joins wait up to one round).
+    // Off by default: on the mixed request stream it did not raise throughput.
+    bool align = false;
     ses_batch batch = nullptr;
+    cudaStream_t stream = nullptr;  // the batch's stream: rounds, joins, observations
 
     std::mutex mu;
-    std::condition_variable cv;    // wakes the worker (new request, cancel, close)
-    std::condition_variable idle;  // signalled whenever nothing is queued or running
+    std::condition_variable cv_admit;   // admitter: new request, memory freed, close
+    std::condition_variable cv_work;    // worker: handle created, cancel, close
+    std::condition_variable cv_finish;  // finisher: request left the batch, close
+    std::condition_variable idle;       // every submitted request has finished
     bool stop = false;
-    std::deque<std::shared_ptr<Request>> queue;
+    bool worker_done = false;
+    std::deque<std::shared_ptr<Request>> queue;     // submitted, waiting for admission
+    std::deque<std::shared_ptr<Request>> created;   // handle built, joins the batch at the next round
+    std::deque<std::shared_ptr<Request>> finished;  // left the batch: read back (if done) and free
     std::map<int64_t, std::shared_ptr<Request>> all;
     int64_t next_id = 1;
-    std::thread worker;
+    int64_t releases = 0;  // handles freed so far (admission retries after out-of-memory)
+    size_t used = 0;       // device bytes charged to admitted requests
+    std::thread worker, admitter, finisher;
 
     // worker-owned
     std::vector<std::shared_ptr<Request>> active;
-    size_t used = 0;
-    cudaStream_t stream = nullptr;              // the batch's stream: rounds, joins, observations
-    cudaEvent_t ev_start[2] = {nullptr, nullptr};  // per round parity: start and end of a queued round
-    cudaEvent_t ev_end[2] = {nullptr, nullptr};
-    ses_observables* obuf[2] = {nullptr, nullptr};  // pinned observable slots per round parity
-    size_t ocap[2] = {0, 0};
 
     // statistics (under mu)
     int64_t submitted = 0, admitted = 0, completed = 0, cancelled = 0, failed = 0, rounds = 0;
     int64_t running = 0;
-    size_t used_view = 0;
     double gridpt_steps = 0, busy_ms = 0;
     std::vector<double> latencies;
     Clock::time_point t_open;
@@ -125,12 +131,19 @@ int next_event(const Request& r) {
     return e;
 }
 
-// Publish a request's final state (worker thread); its handle is released by the caller.
-void publish(ses_server_s* s, const std::shared_ptr<Request>& r, int state, const std::string& err) {
+bool cancelled(ses_server_s* s, const std::shared_ptr<Request>& r) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    return r->cancel;
+}
+
+// Publish a request's final state (counters under the lock); `was_running`: it
+// held a handle (counted in `running`).
+void publish(ses_server_s* s, const std::shared_ptr<Request>& r, int state, const std::string& err,
+             bool was_running) {
     std::lock_guard<std::mutex> lk(s->mu);
     r->state = state;
     r->error = err;
-    --s->running;
+    if (was_running) --s->running;
     if (state == SES_REQ_DONE) {
         r->latency_ms = ms_since(r->t_submit);
         s->latencies.push_back(r->latency_ms);
@@ -140,184 +153,290 @@ void publish(ses_server_s* s, const std::shared_ptr<Request>& r, int state, cons
     } else {
         ++s->failed;
     }
+    s->idle.notify_all();
 }
 
-// Free a request's device memory (leaving the batch first if it is a member).
-void release_handle(ses_server_s* s, const std::shared_ptr<Request>& r) {
-    if (r->h) {
-        ses_gpu_destroy(r->h);  // removes it from the batch when it is a member
-        r->h = nullptr;
-    }
-    s->used -= std::min(s->used, r->bytes);
+// Hand a request that left the batch (or never joined it) to the finisher.
+void to_finisher(ses_server_s* s, const std::shared_ptr<Request>& r, int state, const std::string& err) {
     std::lock_guard<std::mutex> lk(s->mu);
-    s->used_view = s->used;
+    r->final_state = state;
+    r->final_err = err;
+    s->finished.push_back(r);
+    s->cv_finish.notify_one();
 }
 
-void retire(ses_server_s* s, const std::shared_ptr<Request>& r, int state, const std::string& err) {
-    release_handle(s, r);
-    publish(s, r, state, err);
-}
-
-// Create the handle of a queued request (worker thread); it joins the batch
-// later, between rounds.  0: created; 1: out of device memory while other
-// requests hold memory (retry later); 2: failed and published.
-int create_one(ses_server_s* s, const std::shared_ptr<Request>& r, bool others_hold_memory) {
-    ses_handle h = nullptr;
-    ses_status st = ses_gpu_create(&r->grid, r->prec, r->dt, r->mass, r->V.data(), r->psi0.data(), &h);
-    if (st == SES_OK && !r->mx.empty())
-        st = ses_gpu_set_absorber_separable(h, r->mx.data(), r->my.data(), r->mz.data());
-    if (st != SES_OK) {
-        const std::string err = ses_last_error();
-        if (h) ses_gpu_destroy(h);
-        if (st == SES_ENOMEM && others_hold_memory) return 1;
+// ---------------------------------------------------------------------------
+// Admitter thread: creates the handles of queued requests (device allocation,
+// uploads, table builds on the handle's own stream) while the worker keeps the
+// device stepping, first come first served while the estimate fits the budget.
+// ---------------------------------------------------------------------------
+void admitter_main(ses_server_s* s) {
+    cudaSetDevice(s->dev);
+    for (;;) {
+        std::shared_ptr<Request> r;
+        size_t est = 0;
+        int64_t releases_seen = 0;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_admit.wait(lk, [&] {
+                if (s->stop) return true;
+                if (s->queue.empty()) return false;
+                const auto& f = s->queue.front();
+                return f->cancel || estimate_bytes(f->grid, f->prec) + s->used <= s->budget;
+            });
+            if (s->stop) break;
+            r = s->queue.front();
+            s->queue.pop_front();
+            if (r->cancel) {
+                r->state = SES_REQ_CANCELLED;
+                ++s->cancelled;
+                s->idle.notify_all();
+                continue;
+            }
+            est = estimate_bytes(r->grid, r->prec);
+            s->used += est;  // reserved while the handle is built
+            releases_seen = s->releases;
+        }
+        ses_handle h = nullptr;
+        ses_status st = ses_gpu_create(&r->grid, r->prec, r->dt, r->mass, r->V.data(), r->psi0.data(), &h);
+        if (st == SES_OK && !r->mx.empty())
+            st = ses_gpu_set_absorber_separable(h, r->mx.data(), r->my.data(), r->mz.data());
+        if (st != SES_OK) {
+            const std::string err = ses_last_error();
+            if (h) ses_gpu_destroy(h);
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->used -= std::min(s->used, est);
+            if (st == SES_ENOMEM && (s->running > 0 || s->used > 0)) {
+                // others hold device memory: retry once some of it is freed
+                s->queue.push_front(r);
+                s->cv_admit.wait(lk, [&] { return s->stop || s->releases != releases_seen; });
+                continue;
+            }
+            r->state = SES_REQ_FAILED;
+            r->error = err;
+            ++s->failed;
+            s->idle.notify_all();
+            continue;
+        }
+        size_t b = 0;
+        ses_gpu_footprint(h, &b);
         std::lock_guard<std::mutex> lk(s->mu);
-        r->state = SES_REQ_FAILED;
-        r->error = err;
-        ++s->failed;
-        return 2;
+        r->h = h;
+        r->bytes = std::max(b, est);  // charge at least what admission assumed
+        s->used += r->bytes - est;
+        r->V = std::vector<double>();
+        r->psi0 = std::vector<double>();
+        r->state = SES_REQ_RUNNING;
+        ++s->admitted;
+        ++s->running;
+        s->created.push_back(r);
+        s->cv_work.notify_one();
     }
-    size_t b = 0;
-    ses_gpu_footprint(h, &b);
-    r->h = h;
-    r->bytes = std::max(b, estimate_bytes(r->grid, r->prec));  // charge what admission assumed
-    s->used += r->bytes;
-    r->V = std::vector<double>();
-    r->psi0 = std::vector<double>();
-    std::lock_guard<std::mutex> lk(s->mu);
-    r->state = SES_REQ_RUNNING;
-    ++s->admitted;
-    ++s->running;
-    s->used_view = s->used;
-    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Finisher thread: reads back the fields of requests that completed (their own
+// stream waits for the round that finished them), publishes them and frees their
+// handles -- freeing device memory waits for the device, which this thread can
+// afford while the worker keeps rounds queued.
+// ---------------------------------------------------------------------------
+void finisher_main(ses_server_s* s) {
+    cudaSetDevice(s->dev);
+    for (;;) {
+        std::shared_ptr<Request> r;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_finish.wait(lk, [&] { return !s->finished.empty() || s->worker_done; });
+            if (s->finished.empty()) break;  // the worker has exited and nothing is left
+            r = s->finished.front();
+            s->finished.pop_front();
+        }
+        int state = r->final_state;
+        std::string err = r->final_err;
+        if (state == SES_REQ_DONE) {
+            std::vector<double> out((size_t)grid_points(r->grid) * 2);
+            const ses_status rs = ses_gpu_read_psi(r->h, out.data());
+            if (rs != SES_OK) {
+                state = SES_REQ_FAILED;
+                err = ses_last_error();
+            }
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->result.swap(out);
+            r->result_ready = rs == SES_OK;
+        }
+        if (r->h) ses_gpu_destroy(r->h);
+        r->h = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->used -= std::min(s->used, r->bytes);
+            ++s->releases;
+            s->cv_admit.notify_one();
+        }
+        publish(s, r, state, err, true);
+    }
 }
 
 // One queued round: every member advances R merged Strang steps; the listed
-// observers are observed at its end (asynchronously, into pinned slots) and the
-// finishers leave the batch there.
+// observers are observed at its end (asynchronously, into a pinned buffer) and
+// the finishers leave the batch there.
 struct Round {
     int R = 0;
-    int slot = 0;  // pinned observable buffer and event pair (round parity)
-    double pts = 0;
+    double pts = 0;     // grid points x steps
+    double est_ms = 0;  // estimated device time
     std::vector<std::shared_ptr<Request>> observers;
     std::vector<int> obs_step;
     std::vector<std::shared_ptr<Request>> finishers;
+    ses_observables* obs = nullptr;  // pinned, from the worker's pool
+    size_t ocap = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;  // start / end on the server stream, from the pool
 };
 
-// The worker keeps up to two rounds queued on the server's stream, so the
-// device steps round k+1 while the host publishes round k, admits new requests
-// (creates their handles and tables) and reads back finished fields.  Joining,
-// leaving, stepping and observing are all stream-ordered (no host wait); the host
-// waits only for the oldest round's end event.  A round ends at the earliest
-// observation point or completion of any member.
+// Queue rounds until about this much device time is queued: the host's work
+// between rounds then never leaves the device idle, while a newly created
+// request waits at most this long to join.
+constexpr double kQueueMs = 40.0;
+constexpr size_t kMaxQueued = 64;
+
+// ---------------------------------------------------------------------------
+// Worker thread: owns the batch.  Keeps rounds queued on the server's stream --
+// joining, stepping, observing and leaving are all stream-ordered, so the host
+// waits only for the oldest round's end event, then publishes its observations
+// and hands the requests it finished to the finisher.  A round ends at the
+// earliest observation point or completion of any member.
+// ---------------------------------------------------------------------------
 void worker_main(ses_server_s* s) {
     cudaSetDevice(s->dev);
     std::deque<Round> q;
-    std::vector<std::shared_ptr<Request>> pending;  // created, join the batch at the next planned round
-    long long round_no = 0;
-    auto fail_everything = [&](const std::string& err) {
-        for (const auto& r : s->active) retire(s, r, SES_REQ_FAILED, err);
-        s->active.clear();
-        for (Round& rd : q)
-            for (const auto& r : rd.finishers) retire(s, r, SES_REQ_FAILED, err);
-        q.clear();
+    std::vector<std::pair<ses_observables*, size_t>> obs_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    double ms_per_ptstep = 1.0 / 4.0e7;  // device ms per grid point x step, refined from measured rounds
+    double queued_ms = 0.0;
+    long long clock = 0;  // steps planned since the server last ran empty
+    auto give_back = [&](Round& rd) {
+        if (rd.obs) obs_pool.emplace_back(rd.obs, rd.ocap);
+        ev_pool.emplace_back(rd.e0, rd.e1);
+        rd.obs = nullptr;
     };
-    auto cancelled = [&](const std::shared_ptr<Request>& r) {
-        std::lock_guard<std::mutex> lk(s->mu);
-        return r->cancel;
+    auto fail_everything = [&](const std::string& err) {
+        cudaStreamSynchronize(s->stream);
+        for (const auto& r : s->active) {
+            ses_batch_remove(s->batch, r->h);
+            to_finisher(s, r, SES_REQ_FAILED, err);
+        }
+        s->active.clear();
+        for (Round& rd : q) {
+            for (const auto& r : rd.finishers) to_finisher(s, r, SES_REQ_FAILED, err);
+            give_back(rd);
+        }
+        q.clear();
+        queued_ms = 0.0;
     };
     for (;;) {
-        // A. the oldest queued round: wait for its end, publish its observations and results
+        // A. the oldest queued round: wait for its end, publish its observations
         if (!q.empty()) {
             Round rd = std::move(q.front());
             q.pop_front();
-            const cudaEvent_t e1 = s->ev_end[rd.slot];
+            queued_ms = std::max(0.0, queued_ms - rd.est_ms);
             const auto t0 = Clock::now();
             cudaError_t qe;
-            while ((qe = cudaEventQuery(e1)) == cudaErrorNotReady) {
+            while ((qe = cudaEventQuery(rd.e1)) == cudaErrorNotReady) {
                 if (ms_since(t0) > 600000.0) break;
                 std::this_thread::sleep_for(std::chrono::microseconds(20));
             }
-            int derr = 0;
             ses_status st = qe == cudaSuccess ? SES_OK : (qe == cudaErrorNotReady ? SES_ETIMEDOUT : SES_EDEVICE);
             // the batch's error word (an expired bounded wait in a pipelined pass) is
             // read when nothing else is queued, so the check never drains the queue
             if (st == SES_OK && q.empty()) st = ses_batch_sync(s->batch, 600000);
             if (st != SES_OK) {
-                derr = 1;
                 const std::string err = qe == cudaSuccess ? ses_last_error() : "round did not complete";
-                for (const auto& r : rd.finishers) retire(s, r, SES_REQ_FAILED, err);
-                fail_everything(err);
                 cudaGetLastError();
-            }
-            if (!derr) {
+                for (const auto& r : rd.finishers) to_finisher(s, r, SES_REQ_FAILED, err);
+                give_back(rd);
+                fail_everything(err);
+            } else {
                 float ms = 0.0f;
-                cudaEventElapsedTime(&ms, s->ev_start[rd.slot], e1);
+                cudaEventElapsedTime(&ms, rd.e0, rd.e1);
+                if (rd.pts > 0 && ms > 0) ms_per_ptstep = 0.8 * ms_per_ptstep + 0.2 * (ms / rd.pts);
                 {
                     std::lock_guard<std::mutex> lk(s->mu);
                     ++s->rounds;
                     s->gridpt_steps += rd.pts;
                     s->busy_ms += ms;
-                }
-                const ses_observables* ob = s->obuf[rd.slot];
-                for (size_t j = 0; j < rd.observers.size(); ++j) {
-                    Request& r = *rd.observers[j];
-                    const int step = rd.obs_step[j];
-                    ses_record rec{};
-                    rec.id = r.id;
-                    rec.step = step;
-                    rec.final_record = step >= r.nsteps ? 1 : 0;
-                    rec.t_ms = ms_since(r.t_submit);
-                    rec.obs = ob[j];
-                    std::lock_guard<std::mutex> lk(s->mu);
-                    r.records.push_back(rec);
-                }
-                for (const auto& r : rd.finishers) {  // off the batch since this round's end
-                    std::vector<double> out((size_t)grid_points(r->grid) * 2);
-                    const ses_status rs = ses_gpu_read_psi(r->h, out.data());
-                    const std::string err = rs == SES_OK ? "" : ses_last_error();
-                    {
-                        std::lock_guard<std::mutex> lk(s->mu);
-                        r->result.swap(out);
-                        r->result_ready = rs == SES_OK;
+                    for (size_t j = 0; j < rd.observers.size(); ++j) {
+                        Request& r = *rd.observers[j];
+                        ses_record rec{};
+                        rec.id = r.id;
+                        rec.step = rd.obs_step[j];
+                        rec.final_record = rec.step >= r.nsteps ? 1 : 0;
+                        rec.t_ms = ms_since(r.t_submit);
+                        rec.obs = rd.obs[j];
+                        r.records.push_back(rec);
                     }
-                    retire(s, r, rs == SES_OK ? SES_REQ_DONE : SES_REQ_FAILED, err);
                 }
+                give_back(rd);
+                for (const auto& r : rd.finishers) to_finisher(s, r, SES_REQ_DONE, "");
             }
         }
 
-        // B. cancellations of running requests: they leave the batch (stream-ordered) and are freed
+        // B. cancellations of running requests: they leave the batch (stream-ordered)
         for (size_t i = 0; i < s->active.size();) {
-            if (cancelled(s->active[i])) {
+            if (cancelled(s, s->active[i])) {
                 ses_batch_remove(s->batch, s->active[i]->h);
-                retire(s, s->active[i], SES_REQ_CANCELLED, "");
+                to_finisher(s, s->active[i], SES_REQ_CANCELLED, "");
                 s->active.erase(s->active.begin() + (long)i);
             } else {
                 ++i;
             }
         }
 
-        // C. plan and queue rounds until two are in flight
-        while (q.size() < 2) {
-            for (const auto& r : pending) {
-                if (cancelled(r)) {
-                    retire(s, r, SES_REQ_CANCELLED, "");
+        // C. new members join at the next alignment point; rounds are planned and
+        //    queued until about kQueueMs of device work is queued
+        auto join_created = [&]() {
+            std::vector<std::shared_ptr<Request>> joining;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                joining.assign(s->created.begin(), s->created.end());
+                s->created.clear();
+            }
+            for (const auto& r : joining) {
+                if (cancelled(s, r)) {
+                    to_finisher(s, r, SES_REQ_CANCELLED, "");
                     continue;
                 }
                 const ses_status st = ses_batch_add(s->batch, r->h);
                 if (st != SES_OK) {
-                    retire(s, r, SES_REQ_FAILED, ses_last_error());
+                    to_finisher(s, r, SES_REQ_FAILED, ses_last_error());
                     continue;
                 }
                 s->active.push_back(r);
             }
-            pending.clear();
-            if (s->active.empty()) break;
+        };
+        if (s->active.empty()) clock = 0;  // an idle server starts new requests at once
+        const int grid = s->align ? s->max_round : 1;
+        if (clock % grid == 0) join_created();
+        while (!s->active.empty() && q.size() < kMaxQueued && (q.empty() || queued_ms < kQueueMs)) {
+            if (clock % grid == 0 && q.size() > 0) join_created();
             Round rd;
-            rd.slot = (int)(round_no & 1);
-            rd.R = s->max_round;
+            // with alignment, rounds end on the grid of multiples of max_round steps of
+            // the server's clock, where requests join: members that observe every
+            // max_round steps (or a divisor of it) then observe at round ends, and
+            // only completions and other cadences cut rounds short
+            rd.R = s->align ? s->max_round - (int)(clock % s->max_round) : s->max_round;
             for (const auto& r : s->active) rd.R = std::min(rd.R, next_event(*r) - r->done);
             rd.R = std::max(rd.R, 1);
-            cudaEventRecord(s->ev_start[rd.slot], s->stream);
+            clock += rd.R;
+            if (ev_pool.empty()) {
+                cudaEvent_t a = nullptr, b = nullptr;
+                if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+                    fail_everything("event creation failed");
+                    break;
+                }
+                ev_pool.emplace_back(a, b);
+            }
+            rd.e0 = ev_pool.back().first;
+            rd.e1 = ev_pool.back().second;
+            ev_pool.pop_back();
+            cudaEventRecord(rd.e0, s->stream);
             ses_status st = ses_batch_step(s->batch, rd.R, 1);
             for (const auto& r : s->active) {
                 r->done += rd.R;
@@ -327,20 +446,26 @@ void worker_main(ses_server_s* s) {
                     rd.obs_step.push_back(r->done);
                 }
             }
-            if (st == SES_OK && rd.observers.size() > s->ocap[rd.slot]) {
-                if (s->obuf[rd.slot]) cudaFreeHost(s->obuf[rd.slot]);
-                s->obuf[rd.slot] = nullptr;
-                s->ocap[rd.slot] = 0;
-                const size_t want = rd.observers.size() * 2 + 16;
-                if (cudaMallocHost(reinterpret_cast<void**>(&s->obuf[rd.slot]), want * sizeof(ses_observables)) ==
-                    cudaSuccess)
-                    s->ocap[rd.slot] = want;
-                else
-                    st = sfail(SES_ENOMEM, "pinned observable buffer allocation failed");
+            if (st == SES_OK && !rd.observers.empty()) {
+                for (size_t i = 0; i < obs_pool.size(); ++i)
+                    if (obs_pool[i].second >= rd.observers.size()) {
+                        rd.obs = obs_pool[i].first;
+                        rd.ocap = obs_pool[i].second;
+                        obs_pool.erase(obs_pool.begin() + (long)i);
+                        break;
+                    }
+                if (!rd.obs) {
+                    const size_t want = rd.observers.size() * 2 + 16;
+                    if (cudaMallocHost(reinterpret_cast<void**>(&rd.obs), want * sizeof(ses_observables)) ==
+                        cudaSuccess)
+                        rd.ocap = want;
+                    else
+                        st = sfail(SES_ENOMEM, "pinned observable buffer allocation failed");
+                }
             }
             for (size_t j = 0; st == SES_OK && j < rd.observers.size(); ++j) {
                 const Request& r = *rd.observers[j];
-                st = ses_gpu_observe_async(r.h, r.xlo, r.xhi, &s->obuf[rd.slot][j]);
+                st = ses_gpu_observe_async(r.h, r.xlo, r.xhi, &rd.obs[j]);
             }
             for (size_t i = 0; st == SES_OK && i < s->active.size();) {
                 std::shared_ptr<Request> r = s->active[i];
@@ -352,63 +477,35 @@ void worker_main(ses_server_s* s) {
                 }
                 ++i;
             }
-            if (st == SES_OK && cudaEventRecord(s->ev_end[rd.slot], s->stream) != cudaSuccess)
+            if (st == SES_OK && cudaEventRecord(rd.e1, s->stream) != cudaSuccess)
                 st = sfail(SES_EDEVICE, "event record failed");
             if (st != SES_OK) {
                 const std::string err = ses_last_error();
-                for (const auto& r : rd.finishers) retire(s, r, SES_REQ_FAILED, err);
+                for (const auto& r : rd.finishers) to_finisher(s, r, SES_REQ_FAILED, err);
+                give_back(rd);
                 fail_everything(err);
                 break;
             }
+            rd.est_ms = rd.pts * ms_per_ptstep;
+            queued_ms += rd.est_ms;
             q.push_back(std::move(rd));
-            ++round_no;
         }
 
-        // D. admission, first come first served while the estimate fits the budget:
-        //    with rounds queued, a few requests per pass (their set-up overlaps the
-        //    device's work); with nothing to run, one, which then starts stepping
-        std::vector<std::shared_ptr<Request>> take;
-        {
+        // D. nothing queued or running: sleep until a handle is created or the server closes
+        if (q.empty() && s->active.empty()) {
             std::unique_lock<std::mutex> lk(s->mu);
-            if (q.empty() && s->active.empty() && pending.empty() && s->queue.empty()) {
-                s->idle.notify_all();
-                s->cv.wait(lk, [&] { return s->stop || !s->queue.empty(); });
-            }
-            if (s->stop && s->queue.empty() && s->active.empty() && pending.empty() && q.empty()) break;
-            size_t room = s->budget > s->used ? s->budget - s->used : 0;
-            const size_t cap = q.empty() ? 1 : (size_t)kAdmitPerRound;
-            while (!s->queue.empty() && take.size() < cap) {
-                std::shared_ptr<Request> r = s->queue.front();
-                if (r->cancel) {
-                    r->state = SES_REQ_CANCELLED;
-                    ++s->cancelled;
-                    s->queue.pop_front();
-                    continue;
-                }
-                const size_t est = estimate_bytes(r->grid, r->prec);
-                if (est > room) break;
-                room -= est;
-                take.push_back(r);
-                s->queue.pop_front();
-            }
-        }
-        for (size_t i = 0; i < take.size(); ++i) {
-            const bool others = !q.empty() || !s->active.empty() || !pending.empty();
-            const int c = create_one(s, take[i], others);
-            if (c == 0) pending.push_back(take[i]);
-            if (c == 1) {  // out of device memory: back to the head of the queue
-                std::lock_guard<std::mutex> lk(s->mu);
-                for (size_t j = take.size(); j-- > i;) s->queue.push_front(take[j]);
-                break;
-            }
-        }
-        if (q.empty() && s->active.empty() && pending.empty()) {
-            std::lock_guard<std::mutex> lk(s->mu);
-            if (s->queue.empty()) s->idle.notify_all();
+            s->cv_work.wait(lk, [&] { return s->stop || !s->created.empty(); });
+            if (s->stop && s->created.empty()) break;
         }
     }
+    for (auto& o : obs_pool) cudaFreeHost(o.first);
+    for (auto& e : ev_pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
     std::lock_guard<std::mutex> lk(s->mu);
-    s->idle.notify_all();
+    s->worker_done = true;
+    s->cv_finish.notify_all();
 }
 
 double percentile(std::vector<double> v, double p) {
@@ -432,13 +529,11 @@ ses_status ses_serve_open(size_t budget_bytes, int max_round_steps, ses_server* 
     auto* s = new ses_server_s();
     s->budget = budget_bytes;
     s->max_round = max_round_steps > 0 ? max_round_steps : 100;
+    if (const char* e = std::getenv("SES_SERVE_ALIGN")) s->align = std::atoi(e) != 0;
     cudaGetDevice(&s->dev);
     ses_status st = ses_batch_create(&s->batch);
     if (st == SES_OK && cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
         st = sfail(SES_EDEVICE, "stream creation failed");
-    for (int i = 0; st == SES_OK && i < 2; ++i)
-        if (cudaEventCreate(&s->ev_start[i]) != cudaSuccess || cudaEventCreate(&s->ev_end[i]) != cudaSuccess)
-            st = sfail(SES_EDEVICE, "event creation failed");
     if (st == SES_OK) st = ses_batch_set_stream(s->batch, s->stream);
     if (st != SES_OK) {
         if (s->batch) ses_batch_destroy(s->batch);
@@ -448,6 +543,8 @@ ses_status ses_serve_open(size_t budget_bytes, int max_round_steps, ses_server* 
     }
     s->t_open = Clock::now();
     s->worker = std::thread(worker_main, s);
+    s->admitter = std::thread(admitter_main, s);
+    s->finisher = std::thread(finisher_main, s);
     *out = s;
     return SES_OK;
 }
@@ -491,7 +588,7 @@ ses_status ses_serve_submit(ses_server s, const ses_request* r, int64_t* id) {
         s->queue.push_back(q);
         ++s->submitted;
     }
-    s->cv.notify_one();
+    s->cv_admit.notify_one();
     *id = q->id;
     return SES_OK;
 }
@@ -538,7 +635,8 @@ ses_status ses_serve_cancel(ses_server s, int64_t id) {
         if (it == s->all.end()) return sfail(SES_ENOTFOUND, "unknown request id");
         it->second->cancel = true;
     }
-    s->cv.notify_one();
+    s->cv_admit.notify_all();
+    s->cv_work.notify_all();
     return SES_OK;
 }
 
@@ -564,7 +662,7 @@ ses_status ses_serve_stats(ses_server s, ses_serve_stats_t* out) {
     out->queued = (int64_t)s->queue.size();
     out->running = s->running;
     out->rounds = s->rounds;
-    out->bytes_in_use = s->used_view;
+    out->bytes_in_use = s->used;
     out->budget = s->budget;
     out->gridpt_steps = s->gridpt_steps;
     out->busy_ms = s->busy_ms;
@@ -581,17 +679,17 @@ ses_status ses_serve_close(ses_server s) {
         s->stop = true;
         for (auto& kv : s->all) kv.second->cancel = true;
     }
-    s->cv.notify_all();
-    if (s->worker.joinable()) s->worker.join();
-    for (auto& r : s->active)
-        if (r->h) ses_gpu_destroy(r->h);
+    s->cv_admit.notify_all();
+    s->cv_work.notify_all();
+    if (s->admitter.joinable()) s->admitter.join();  // a handle being built lands in `created`
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->cv_work.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();      // cancels the running requests, drains its rounds
+    if (s->finisher.joinable()) s->finisher.join();  // frees every handle
     ses_batch_destroy(s->batch);
     cudaStreamSynchronize(s->stream);
-    for (int i = 0; i < 2; ++i) {
-        if (s->ev_start[i]) cudaEventDestroy(s->ev_start[i]);
-        if (s->ev_end[i]) cudaEventDestroy(s->ev_end[i]);
-        if (s->obuf[i]) cudaFreeHost(s->obuf[i]);
-    }
     cudaStreamDestroy(s->stream);
     delete s;
     return SES_OK;
