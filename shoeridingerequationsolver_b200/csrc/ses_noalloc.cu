@@ -6,6 +6,7 @@
 // latency-critical loop that must not pay cudaMalloc/cudaFree's device-wide
 // synchronisation.  The caller passes psi, V and the output in its own device
 // memory; the per-CTA partial sums live in a fixed file-scope device array.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -54,11 +55,11 @@ __global__ void __launch_bounds__(kNoAllocThreads)
 #pragma unroll 4
     for (int it = 0; it < kNoAllocPerThread; ++it) {
         const long long idx = base + (long long)it * kNoAllocThreads + threadIdx.x;
-        if (idx < o.N) {
-            const long long line = idx / o.nx;
-            const int i = (int)(idx - line * o.nx);
-            const long long k = line / o.ny;
-            const int j = (int)(line - k * o.ny);
+        if (idx < o.N) {  // N <= 2^27: the 32-bit division by invariant integers applies
+            const uint32_t line = fdiv((uint32_t)idx, o.fnx);
+            const int i = (int)(idx - (long long)line * o.nx);
+            const uint32_t k = fdiv(line, o.fny);
+            const int j = (int)(line - k * (uint32_t)o.ny);
             const cx<double> p = widen(psi[idx]);
             const double w = p.x * p.x + p.y * p.y;
             const double x = o.x0 + i * o.hx, y = o.y0 + j * o.hy, z = o.z0 + (double)k * o.hz;
@@ -103,15 +104,38 @@ __global__ void __launch_bounds__(kNoAllocThreads)
     }
 }
 
-// Device address of the scratch array, resolved once per device with that
-// device current (the host-side symbol is only a stand-in for it).
+// Device address of the scratch array, resolved once per device and context with
+// that device current (the host-side symbol is only a stand-in for it).  The
+// cache is keyed by the current context as well as the ordinal: after a device
+// reset the library's module is loaded again into a new context, at a new
+// address, which is then resolved afresh.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+CUcontext current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (CtxGetCurrentFn) nullptr;
+        }
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    CUcontext c = nullptr;
+    if (fn) fn(&c);
+    return c;
+}
+
 std::mutex g_mu;
 void* g_addr[64] = {nullptr};
+CUcontext g_ctx[64] = {nullptr};
 
 ses_status scratch_address(int dev, unsigned char** out) {
     if (dev < 0 || dev >= 64) return nfail(SES_EINVAL, "device ordinal out of range");
+    const CUcontext ctx = current_context();
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    if (!g_addr[dev] || g_ctx[dev] != ctx) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -120,6 +144,7 @@ ses_status scratch_address(int dev, unsigned char** out) {
                                           cudaGetErrorString(e));
         }
         g_addr[dev] = p;
+        g_ctx[dev] = ctx;
     }
     *out = static_cast<unsigned char*>(g_addr[dev]);
     return SES_OK;
@@ -161,6 +186,8 @@ extern "C" ses_status ses_observe_real_noalloc(const ses_grid_desc* grid, ses_pr
     o.N = N;
     o.nx = ax[0].n;
     o.ny = ax[1].n;
+    o.fnx = make_fastdiv((uint32_t)o.nx);
+    o.fny = make_fastdiv((uint32_t)o.ny);
     o.x0 = ax[0].xmin;
     o.hx = (ax[0].xmax - ax[0].xmin) / ax[0].n;
     o.y0 = ax[1].xmin;
