@@ -16,7 +16,14 @@ import ctypes as C
 import numpy as np
 import pytest
 
-TOL = 1e-12  # all reduce the same values in FP64; only the summation order differs
+TOL = 1e-12  # the device reductions: the same values in FP64, only the blocked summation order differs
+
+
+def tol_oracle(npts):
+    """The oracle sums left to right (core/src/field.ixx:68-74), whose rounding grows
+    with the point count (about sqrt(N) ulps): 1e-11 relative at 65536 points,
+    scaled by sqrt(N / 65536) above."""
+    return 1e-11 * max(1.0, (npts / 65536.0) ** 0.5)
 
 
 def _grid(ses, box, n):
@@ -76,7 +83,8 @@ def test_noalloc_matches_oracle_and_observe_on_two_calls(ses, oracle, prec, case
         assert np.allclose(got, expect, rtol=TOL, atol=TOL), (call, got, expect)
         # the oracle: norm, probability and moments; <V> against the FP64 sum of V |psi|^2 / sum |psi|^2
         idx = [0, 2, 3, 4, 5, 6, 7, 8]
-        assert np.allclose(got[idx], want[idx], rtol=TOL, atol=TOL), (call, got[idx], want[idx])
+        to = tol_oracle(n[0] * n[1] * n[2])
+        assert np.allclose(got[idx], want[idx], rtol=to, atol=to), (call, got[idx], want[idx])
         w = field.real ** 2 + field.imag ** 2
         assert abs(got[1] - float(np.sum(V * w) / np.sum(w))) <= 1e-12 * max(1.0, abs(got[1]))
     # without a potential: <V> is 0, the other eight values are unchanged
