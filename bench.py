@@ -66,7 +66,8 @@ def parse_args(argv=None):
     ap.add_argument("--instances", type=int, default=256, help="batched sweep size per GPU (c4)")
     ap.add_argument("--sizes", default="", help="c4: keep only these grid sizes (comma list), for profiling")
     ap.add_argument("--n", type=int, default=0, help="grid size override for c1/c2/c3")
-    ap.add_argument("--precision", choices=["c64", "c128"], default="c64")
+    ap.add_argument("--precision", choices=["c64", "c128"], default=None,
+                    help="c1/c2/c3 line precision (default: c128 for c1, the plain FP64 config; else c64)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg and its parity checks")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity checks of the CPU leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving run")
@@ -886,6 +887,8 @@ NO_AUTOTUNE = False
 def main(argv=None):
     global NO_AUTOTUNE
     args = parse_args(argv)
+    if args.precision is None:
+        args.precision = "c128" if args.config == "c1" else "c64"
     NO_AUTOTUNE = args.no_autotune
     if args.impl == "reference":
         return run_reference(args)
