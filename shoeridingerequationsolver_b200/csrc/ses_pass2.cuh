@@ -206,9 +206,14 @@ struct XShape {
 // vt (optional): shared memory for this CTA's potential-table rows (NW * LPW
 // lines of N entries); the between-steps and batch-end passes then fetch the
 // rows asynchronously at the start of the tile and read them after the first FFT.
-template <typename T, int MODE, int N, int E, int R0, int R1, int R2, class A>
+// FASTKICK (between-steps pass of the batched kernel only): the pass applies the
+// full kick with a separable absorber from staged table and profile rows -- the
+// run-time tests of the general path (table kind, mask kind, staged rows) are
+// resolved at compile time, leaving straight-line code per element.
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, bool FASTKICK = false, class A>
 __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb, const cx<T>* twh,
                                             const cx<T>* twl, cx<T>* vt = nullptr) {
+    static_assert(!FASTKICK || MODE == XM_MID, "the fast kick is the between-steps pass");
     using XS = XShape<T, N, E>;
     constexpr int TL = XS::TL;
     constexpr int LPW = XS::LPW;
@@ -255,9 +260,9 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
             v[b * RF + r] = kConjIn ? cconj(e) : e;
         }
     if constexpr (kTabLate) {
-        const bool want = MODE == XM_MID ? a.d_mid != DG_NONE : a.d_store != DG_NONE;
-        const bool wantm = (MODE == XM_MID ? a.m_mid : a.m_store) && !mfull && mx;
-        if (vt && (want || wantm)) {  // this warp's rows, 16-byte chunks spread over the lanes
+        const bool want = FASTKICK || (MODE == XM_MID ? a.d_mid != DG_NONE : a.d_store != DG_NONE);
+        const bool wantm = FASTKICK || ((MODE == XM_MID ? a.m_mid : a.m_store) && !mfull && mx);
+        if (FASTKICK || (vt && (want || wantm))) {  // this warp's rows, 16-byte chunks spread over the lanes
             __syncwarp();  // the previous tile's reads of these rows are done
             if (want) {  // line by line, lane-strided 16-byte chunks: constant offsets per copy
                 constexpr int CH = N * (int)sizeof(cx<T>) / 16;
@@ -301,7 +306,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
     rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, twh, twl, x);
     // v[b*RL + r] now at position q + TL b + r N/RL
     if constexpr (kTabLate) {
-        if (vt) {
+        if (FASTKICK || vt) {
             cp_async_wait_all();
             __syncwarp();
         }
@@ -352,7 +357,10 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
             for (int r = 0; r < RL; ++r) {
                 const int pos = q + TL * b + r * (N / RL);
                 cx<T> e = v[b * RL + r];
-                if constexpr (MODE == XM_MID) {
+                if constexpr (MODE == XM_MID && FASTKICK) {
+                    // (psi h (m)) h with the staged row h and profile mx, m = mx[pos] my[j] mz[k]
+                    e = apply_diag_tv(cconj(e), DG_FULL, vrow[pos], 1, ms[pos] * myz);
+                } else if constexpr (MODE == XM_MID) {
                     e = cconj(e);
                     if (a.d_mid != DG_NONE || a.m_mid) e = diag(e, a.d_mid, a.m_mid, pos);
                 } else if (a.tb.kfull) {  // long line: kinetic of frequency k2 + N2 k1
@@ -578,7 +586,16 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, XShape<T, N, E>::MIN
     __syncthreads();
     for (uint32_t t = blockIdx.x; t < w.total; t += gridDim.x) {
         const uint32_t inst = fdiv(t, w.fbpi);
-        xpass2_body<T, MODE, N, E, R0, R1, R2>(args[inst], (long long)(t - inst * w.bpi), xb, tw, TW::lo_of(tw), vt);
+        const PassArgs<T>& a = args[inst];
+        if constexpr (MODE == XM_MID) {
+            // the common between-steps program: full kick and a separable absorber
+            if (a.d_mid == DG_FULL && a.m_mid && a.tb.maskfull == nullptr && a.tb.mask1[0] != nullptr) {
+                xpass2_body<T, MODE, N, E, R0, R1, R2, true>(a, (long long)(t - inst * w.bpi), xb, tw, TW::lo_of(tw),
+                                                             vt);
+                continue;
+            }
+        }
+        xpass2_body<T, MODE, N, E, R0, R1, R2>(a, (long long)(t - inst * w.bpi), xb, tw, TW::lo_of(tw), vt);
     }
 }
 
