@@ -361,22 +361,37 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                     }
             }
         } else if constexpr (MODE == XM_MID || MODE == XM_1D) {
-            const cx<double> dyz = dmul1(a.tb.kd[1][jy], a.tb.kd[2][kz]);
+            // the common between-steps program -- full kick, separable absorber -- as
+            // straight-line code (the same arithmetic as the general path below)
+            bool fast = false;
+            if constexpr (MODE == XM_MID) fast = a.d_mid == DG_FULL && a.m_mid && sep;
+            if (fast) {
 #pragma unroll
-            for (int b = 0; b < E / RL; ++b)
+                for (int b = 0; b < E / RL; ++b)
 #pragma unroll
-                for (int r = 0; r < RL; ++r) {
-                    const int pos = q + TL * b + r * (N / RL);
-                    cx<T> e = v[b * RL + r];
-                    if constexpr (MODE == XM_MID) {
-                        e = cconj(e);
-                        if (a.d_mid != DG_NONE || a.m_mid)
-                            e = apply_diag_tv(e, a.d_mid, tline[pos], a.m_mid, a.m_mid ? mval(pos) : 1.0);
-                    } else {
-                        e = kinetic_conj(e, dmul1(dyz, a.tb.kd[0][pos]), a.tb.kscale);
+                    for (int r = 0; r < RL; ++r) {
+                        const int pos = q + TL * b + r * (N / RL);
+                        const double m = (kTab ? mrow[pos] : a.tb.mask1[0][pos]) * myz;
+                        v[b * RL + r] = apply_diag_tv(cconj(v[b * RL + r]), DG_FULL, tline[pos], 1, m);
                     }
-                    v[b * RL + r] = e;
-                }
+            } else {
+                const cx<double> dyz = dmul1(a.tb.kd[1][jy], a.tb.kd[2][kz]);
+#pragma unroll
+                for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const int pos = q + TL * b + r * (N / RL);
+                        cx<T> e = v[b * RL + r];
+                        if constexpr (MODE == XM_MID) {
+                            e = cconj(e);
+                            if (a.d_mid != DG_NONE || a.m_mid)
+                                e = apply_diag_tv(e, a.d_mid, tline[pos], a.m_mid, a.m_mid ? mval(pos) : 1.0);
+                        } else {
+                            e = kinetic_conj(e, dmul1(dyz, a.tb.kd[0][pos]), a.tb.kscale);
+                        }
+                        v[b * RL + r] = e;
+                    }
+            }
             rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
             if (valid) {
 #pragma unroll
