@@ -15,16 +15,25 @@
 
 namespace sesk {
 
-template <typename T>
+// PK (complex64): hi points to the interleaved table {h.x, h.y, l.x, l.y} per
+// entry (the shared-memory copy), read with one 16-byte load; lo is unused.
+template <typename T, bool PK = false>
 __device__ __forceinline__ cx<T> twmul(cx<T> v, const cx<T>* __restrict__ hi,
                                        const cx<T>* __restrict__ lo, int idx) {
-    const cx<T> h = hi[idx];
     if constexpr (sizeof(T) == 4) {  // compensated: v * (h + l), l = FP32 remainder of the FP64 twiddle
-        const cx<T> l = lo[idx];
+        cx<T> h, l;
+        if constexpr (PK) {
+            const float4 t = reinterpret_cast<const float4*>(hi)[idx];
+            h = mk<float>(t.x, t.y);
+            l = mk<float>(t.z, t.w);
+        } else {
+            h = hi[idx];
+            l = lo[idx];
+        }
         return mk<T>(fmaf(v.x, h.x, fmaf(-v.y, h.y, fmaf(v.x, l.x, -v.y * l.y))),
                      fmaf(v.x, h.y, fmaf(v.y, h.x, fmaf(v.x, l.y, v.y * l.x))));
     } else {
-        return v * h;
+        return v * hi[idx];
     }
 }
 
@@ -47,7 +56,7 @@ __device__ __forceinline__ cx<T> tw4_mul(cx<T> v, const Tables& tb, long long f)
 // One Stockham stage of radix R after NS points per butterfly group: twiddle
 // then DFT of each of the thread's E/R butterflies.  A stage's table holds
 // R x NS entries, w^{r k N/(NS R)} at [OFF + r*NS + k].
-template <typename T, int N, int E, int TL, int R, int NS, int OFF>
+template <typename T, int N, int E, int TL, int R, int NS, int OFF, bool PK = false>
 __device__ __forceinline__ void rstage(cx<T> (&v)[E], int q, const cx<T>* __restrict__ twh,
                                        const cx<T>* __restrict__ twl) {
     constexpr int B = E / R;
@@ -56,7 +65,7 @@ __device__ __forceinline__ void rstage(cx<T> (&v)[E], int q, const cx<T>* __rest
         if constexpr (NS > 1) {
             const int k = (q + TL * b) % NS;
 #pragma unroll
-            for (int r = 1; r < R; ++r) v[b * R + r] = twmul(v[b * R + r], twh, twl, OFF + r * NS + k);
+            for (int r = 1; r < R; ++r) v[b * R + r] = twmul<T, PK>(v[b * R + r], twh, twl, OFF + r * NS + k);
         }
         dft<T, R>(&v[b * R]);
     }
@@ -84,17 +93,17 @@ __device__ __forceinline__ void rexchange(cx<T> (&v)[E], int q, X& x) {
 
 // Forward FFT of plan (R0, R1, R2) (R = 1: stage absent), tables of that plan.
 // In:  v[b*R0 + r] = x[q + TL b + r N/R0].   Out: v[b*RL + r] = X[q + TL b + r N/RL].
-template <typename T, int N, int E, int R0, int R1, int R2, int TOFF, class X>
+template <typename T, int N, int E, int R0, int R1, int R2, int TOFF, bool PK = false, class X>
 __device__ __forceinline__ void rfft(cx<T> (&v)[E], int q, const cx<T>* twh, const cx<T>* twl, X& x) {
     constexpr int TL = N / E;
-    rstage<T, N, E, TL, R0, 1, TOFF>(v, q, twh, twl);
+    rstage<T, N, E, TL, R0, 1, TOFF, PK>(v, q, twh, twl);
     if constexpr (R1 > 1) {
         rexchange<T, N, E, TL, R0, 1, R1>(v, q, x);
-        rstage<T, N, E, TL, R1, R0, TOFF + R0>(v, q, twh, twl);
+        rstage<T, N, E, TL, R1, R0, TOFF + R0, PK>(v, q, twh, twl);
     }
     if constexpr (R2 > 1) {
         rexchange<T, N, E, TL, R1, R0, R2>(v, q, x);
-        rstage<T, N, E, TL, R2, R0 * R1, TOFF + R0 + R1 * R0>(v, q, twh, twl);
+        rstage<T, N, E, TL, R2, R0 * R1, TOFF + R0 + R1 * R0, PK>(v, q, twh, twl);
     }
 }
 
@@ -110,32 +119,36 @@ struct PlanShape {
     static constexpr int tables = fwd_tables + rev_tables;
 };
 
-// Shared-memory copy of a plan's stage twiddles (forward then reversed tables;
-// complex64 also the lo parts) for persistent kernels: loaded once per CTA, so
-// the FFT stages read twiddles at shared-memory latency and the tables of
-// many instances do not compete for L1.
+// Shared-memory copy of a plan's stage twiddles (forward then reversed tables)
+// for persistent kernels: loaded once per CTA, so the FFT stages read twiddles at
+// shared-memory latency and the tables of many instances do not compete for L1.
+// complex64 entries are interleaved {h.x, h.y, l.x, l.y} (hi part and FP32
+// remainder), 16 bytes each, read by twmul<float, true> with one load.  The copy
+// must start on a 16-byte boundary.
 template <typename T, int R0, int R1, int R2>
 struct TwStage {
     static constexpr int count = PlanShape<R0, R1, R2>::tables;
     static constexpr size_t bytes = (size_t)count * sizeof(cx<T>) * (sizeof(T) == 4 ? 2 : 1);
     static __device__ __forceinline__ void load(cx<T>* dst, const cx<T>* hi, const cx<T>* lo) {
         for (int i = threadIdx.x; i < count; i += blockDim.x) {
-            dst[i] = hi[i];
-            if constexpr (sizeof(T) == 4) dst[count + i] = lo[i];
+            if constexpr (sizeof(T) == 4)
+                reinterpret_cast<float4*>(dst)[i] = make_float4(hi[i].x, hi[i].y, lo[i].x, lo[i].y);
+            else
+                dst[i] = hi[i];
         }
     }
-    static __device__ __forceinline__ const cx<T>* lo_of(const cx<T>* dst) {
-        return sizeof(T) == 4 ? dst + count : dst;
-    }
+    // the twl argument that goes with the copy (unused by the interleaved reads)
+    static __device__ __forceinline__ const cx<T>* lo_of(const cx<T>* dst) { return dst; }
 };
 
 // FFT with the plan's own order (tables at 0) or reversed order (tables after).
-template <typename T, int N, int E, int R0, int R1, int R2, bool REV, class X>
+// PK: the tables are the interleaved shared-memory copy of TwStage.
+template <typename T, int N, int E, int R0, int R1, int R2, bool REV, bool PK = false, class X>
 __device__ __forceinline__ void rfft_plan(cx<T> (&v)[E], int q, const cx<T>* twh, const cx<T>* twl,
                                           X& x) {
     using S = PlanShape<R0, R1, R2>;
-    if constexpr (!REV) rfft<T, N, E, R0, R1, R2, 0>(v, q, twh, twl, x);
-    else rfft<T, N, E, S::v0, S::v1, S::v2, S::fwd_tables>(v, q, twh, twl, x);
+    if constexpr (!REV) rfft<T, N, E, R0, R1, R2, 0, PK>(v, q, twh, twl, x);
+    else rfft<T, N, E, S::v0, S::v1, S::v2, S::fwd_tables, PK>(v, q, twh, twl, x);
 }
 
 // Padded line in shared memory: element pos at pos + PM * (pos >> SH).
@@ -210,7 +223,8 @@ struct XShape {
 // full kick with a separable absorber from staged table and profile rows -- the
 // run-time tests of the general path (table kind, mask kind, staged rows) are
 // resolved at compile time, leaving straight-line code per element.
-template <typename T, int MODE, int N, int E, int R0, int R1, int R2, bool FASTKICK = false, class A>
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, bool FASTKICK = false, bool PK = false,
+          class A>
 __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb, const cx<T>* twh,
                                             const cx<T>* twl, cx<T>* vt = nullptr) {
     static_assert(!FASTKICK || MODE == XM_MID, "the fast kick is the between-steps pass");
@@ -303,7 +317,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
         return apply_diag(e, kind, msk, f, pos, jy, kz, a.tb);
     };
 
-    rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, twh, twl, x);
+    rfft_plan<T, N, E, R0, R1, R2, kRev, PK>(v, q, twh, twl, x);
     // v[b*RL + r] now at position q + TL b + r N/RL
     if constexpr (kTabLate) {
         if (FASTKICK || vt) {
@@ -370,7 +384,7 @@ __device__ __forceinline__ void xpass2_body(const A& a, long long blk, cx<T>* xb
                 }
                 v[b * RL + r] = e;
             }
-        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
+        rfft_plan<T, N, E, R0, R1, R2, true, PK>(v, q, twh, twl, x);
         // v[b*R0 + r] at position q + TL b + r N/R0
         if (valid) {
 #pragma unroll
@@ -402,7 +416,7 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, XShape<T, N, E>::MIN
 // Strided-axis (y or z) pass, compiled plan.  CTA = L lines x N/E threads per
 // line; thread (l = tid % L, q = tid / L).  Modes as in SModeK.
 // ---------------------------------------------------------------------------
-template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, class A>
+template <typename T, int MODE, int N, int E, int R0, int R1, int R2, int L, bool PK = false, class A>
 __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* tile, const cx<T>* twh,
                                             const cx<T>* twl) {
     constexpr int TL = N / E;
@@ -451,7 +465,7 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
             v[b * RF + r] = e;
         }
 
-    rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, twh, twl, x);
+    rfft_plan<T, N, E, R0, R1, R2, kRev, PK>(v, q, twh, twl, x);
 
     if constexpr (MODE == SM_TW_START || MODE == SM_TW_END) {
         if (valid) {
@@ -482,7 +496,7 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
                 if (a.d_mid != DG_NONE || a.m_mid) e = diag(e, a.d_mid, a.m_mid, pos);
                 v[b * RL + r] = e;
             }
-        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
+        rfft_plan<T, N, E, R0, R1, R2, true, PK>(v, q, twh, twl, x);
         if (valid) {
 #pragma unroll
             for (int b = 0; b < E / R0; ++b)
@@ -539,7 +553,7 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
                 const int pos = q + TL * b + r * (N / RL);
                 v[b * RL + r] = kinetic_apply(v[b * RL + r], dother, kda, kdaf, pos, a.tb.kscale);
             }
-        rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
+        rfft_plan<T, N, E, R0, R1, R2, true, PK>(v, q, twh, twl, x);
         if (valid) {
 #pragma unroll
             for (int b = 0; b < E / R0; ++b)
@@ -590,12 +604,14 @@ __global__ void __launch_bounds__(XShape<T, N, E>::NW * 32, XShape<T, N, E>::MIN
         if constexpr (MODE == XM_MID) {
             // the common between-steps program: full kick and a separable absorber
             if (a.d_mid == DG_FULL && a.m_mid && a.tb.maskfull == nullptr && a.tb.mask1[0] != nullptr) {
-                xpass2_body<T, MODE, N, E, R0, R1, R2, true>(a, (long long)(t - inst * w.bpi), xb, tw, TW::lo_of(tw),
+                xpass2_body<T, MODE, N, E, R0, R1, R2, true, true>(a, (long long)(t - inst * w.bpi), xb, tw,
+                                                                   TW::lo_of(tw),
                                                              vt);
                 continue;
             }
         }
-        xpass2_body<T, MODE, N, E, R0, R1, R2>(a, (long long)(t - inst * w.bpi), xb, tw, TW::lo_of(tw), vt);
+        xpass2_body<T, MODE, N, E, R0, R1, R2, false, true>(a, (long long)(t - inst * w.bpi), xb, tw, TW::lo_of(tw),
+                                                            vt);
     }
 }
 
@@ -620,7 +636,8 @@ __global__ void __launch_bounds__(L*(N / E), 1)
     __syncthreads();
     for (uint32_t t = blockIdx.x; t < w.total; t += gridDim.x) {
         const uint32_t inst = fdiv(t, w.fbpi);
-        spass2_body<T, MODE, N, E, R0, R1, R2, L>(args[inst], (long long)(t - inst * w.bpi), tile, tw, TW::lo_of(tw));
+        spass2_body<T, MODE, N, E, R0, R1, R2, L, true>(args[inst], (long long)(t - inst * w.bpi), tile, tw,
+                                                        TW::lo_of(tw));
     }
 }
 

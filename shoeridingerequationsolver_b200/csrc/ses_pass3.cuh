@@ -154,7 +154,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
                 v[b * R0 + r] = MODE == SM_INV ? cconj(e) : e;
             }
         __syncthreads();  // all stage-0 reads before the tile is reused for exchanges
-        rfft_plan<T, N, E, R0, R1, R2, false>(v, q, twh, twl, x);
+        rfft_plan<T, N, E, R0, R1, R2, false, kSmemTw>(v, q, twh, twl, x);
 
         int c1, c2;
         if (ypass) {
@@ -187,7 +187,7 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
                     const int pos = q + TL * b + r * (N / RL);
                     v[b * RL + r] = kinetic_apply(v[b * RL + r], dother, kda, kdaf, pos, a.tb.kscale);
                 }
-            rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
+            rfft_plan<T, N, E, R0, R1, R2, true, kSmemTw>(v, q, twh, twl, x);
             if (valid) {
 #pragma unroll
                 for (int b = 0; b < E / R0; ++b)
@@ -341,7 +341,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                 v[b * RF + r] = kConjIn ? cconj(e) : e;
             }
         __syncwarp();  // the line is reused for exchanges: all stage-0 reads first
-        rfft_plan<T, N, E, R0, R1, R2, kRev>(v, q, twh, twl, x);
+        rfft_plan<T, N, E, R0, R1, R2, kRev, kSmemTw>(v, q, twh, twl, x);
 
         if constexpr (MODE == XM_FWD || MODE == XM_START || MODE == XM_END) {
             if (valid) {
@@ -392,7 +392,7 @@ __device__ __forceinline__ void xpass3_body(const F& f, const PipeArgs& pa) {
                         v[b * RL + r] = e;
                     }
             }
-            rfft_plan<T, N, E, R0, R1, R2, true>(v, q, twh, twl, x);
+            rfft_plan<T, N, E, R0, R1, R2, true, kSmemTw>(v, q, twh, twl, x);
             if (valid) {
 #pragma unroll
                 for (int b = 0; b < E / R0; ++b)
