@@ -18,9 +18,9 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libses_b200.so"
 SOURCES = ["ses_gpu.cu", "ses_plans_small.cu", "ses_plans_mixed.cu", "ses_plans_256.cu",
-           "ses_plans_large.cu", "ses_noalloc.cu", "ses_serve.cpp"]
+           "ses_plans_large.cu", "ses_plans_plane.cu", "ses_noalloc.cu", "ses_serve.cpp"]
 HEADERS = ["ses_fft.cuh", "ses_pass.cuh", "ses_pass2.cuh", "ses_pass3.cuh", "ses_tma.cuh", "ses_plans.cuh", "ses_engine.cuh",
-           "ses_aux.cuh"]
+           "ses_aux.cuh", "ses_plane.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-shared",

@@ -51,9 +51,13 @@ __device__ __forceinline__ cx<float> operator-(cx<float> a, cx<float> b) {
         : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
     return c;
 }
+// Complex product with the FMAs written out: the compiler may not contract the
+// two products of a component differently in different kernels, so every pass
+// that multiplies the same operands gets the same bits (a run split into two
+// calls equals one call; the step forms agree).
 template <typename T>
 __device__ __forceinline__ cx<T> operator*(cx<T> a, cx<T> b) {
-    return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return mk<T>(fma(a.x, b.x, -(a.y * b.y)), fma(a.x, b.y, a.y * b.x));
 }
 // a * s for an FP64 scale s such as 1/N, which is not a power of two for
 // radix-3/5 sizes: complex64 carries s as hi + lo, so that the scale applied
@@ -147,7 +151,7 @@ __device__ __forceinline__ cx<T> rotc(cx<T> v, CK<T> c, CK<T> s) {
         return mk<T>(fmaf(v.x, c.hi, fmaf(v.y, s.hi, fmaf(v.x, c.lo, v.y * s.lo))),
                      fmaf(v.y, c.hi, fmaf(-v.x, s.hi, fmaf(v.y, c.lo, -v.x * s.lo))));
     } else {
-        return mk<T>(v.x * c.hi + v.y * s.hi, v.y * c.hi - v.x * s.hi);
+        return mk<T>(fma(v.x, c.hi, v.y * s.hi), fma(v.y, c.hi, -(v.x * s.hi)));
     }
 }
 
@@ -268,10 +272,17 @@ __device__ __forceinline__ void dft3(cx<T>* v) {
         m = from_f2(__ffma2_rn(as_f2(t), make_float2(-0.5f, -0.5f), as_f2(v[0])));
     else
         m = mk<T>(fma(-0.5, t.x, v[0].x), fma(-0.5, t.y, v[0].y));
-    const cx<T> d = kmulc(v[1] - v[2], hs3);
-    v[0] = v[0] + t;
-    v[1] = mk<T>(m.x + d.y, m.y - d.x);  // m - i d
-    v[2] = mk<T>(m.x - d.y, m.y + d.x);  // m + i d
+    if constexpr (sizeof(T) == 4) {
+        const cx<T> d = kmulc(v[1] - v[2], hs3);
+        v[0] = v[0] + t;
+        v[1] = mk<T>(m.x + d.y, m.y - d.x);  // m - i d
+        v[2] = mk<T>(m.x - d.y, m.y + d.x);  // m + i d
+    } else {  // d = (v1 - v2) sin(2 pi/3), folded into explicit FMAs
+        const cx<T> b = v[1] - v[2];
+        v[0] = v[0] + t;
+        v[1] = mk<T>(fma(b.y, hs3.hi, m.x), fma(-b.x, hs3.hi, m.y));
+        v[2] = mk<T>(fma(-b.y, hs3.hi, m.x), fma(b.x, hs3.hi, m.y));
+    }
 }
 
 template <typename T>
@@ -282,10 +293,18 @@ __device__ __forceinline__ void dft5(cx<T>* v) {
     const CK<T> s2 = ck<T>(0.58778525229247312917);   // sin(4 pi/5)
     const cx<T> a1 = v[1] + v[4], a2 = v[2] + v[3];
     const cx<T> b1 = v[1] - v[4], b2 = v[2] - v[3];
-    const cx<T> p1 = v[0] + kmulc(a1, c1) + kmulc(a2, c2);
-    const cx<T> p2 = v[0] + kmulc(a1, c2) + kmulc(a2, c1);
-    const cx<T> q1 = kmulc(b1, s1) + kmulc(b2, s2);
-    const cx<T> q2 = kmulc(b1, s2) - kmulc(b2, s1);
+    cx<T> p1, p2, q1, q2;
+    if constexpr (sizeof(T) == 4) {
+        p1 = v[0] + kmulc(a1, c1) + kmulc(a2, c2);
+        p2 = v[0] + kmulc(a1, c2) + kmulc(a2, c1);
+        q1 = kmulc(b1, s1) + kmulc(b2, s2);
+        q2 = kmulc(b1, s2) - kmulc(b2, s1);
+    } else {  // the same sums with the FMAs written out
+        p1 = mk<T>(fma(a2.x, c2.hi, fma(a1.x, c1.hi, v[0].x)), fma(a2.y, c2.hi, fma(a1.y, c1.hi, v[0].y)));
+        p2 = mk<T>(fma(a2.x, c1.hi, fma(a1.x, c2.hi, v[0].x)), fma(a2.y, c1.hi, fma(a1.y, c2.hi, v[0].y)));
+        q1 = mk<T>(fma(b1.x, s1.hi, b2.x * s2.hi), fma(b1.y, s1.hi, b2.y * s2.hi));
+        q2 = mk<T>(fma(b1.x, s2.hi, -(b2.x * s1.hi)), fma(b1.y, s2.hi, -(b2.y * s1.hi)));
+    }
     v[0] = v[0] + a1 + a2;
     v[1] = mk<T>(p1.x + q1.y, p1.y - q1.x);  // p1 - i q1
     v[4] = mk<T>(p1.x - q1.y, p1.y + q1.x);  // p1 + i q1

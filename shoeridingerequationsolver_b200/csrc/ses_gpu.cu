@@ -25,6 +25,7 @@
 #include "ses_engine.cuh"
 #include "ses_pass.cuh"
 #include "ses_plans.cuh"
+#include "ses_plane.cuh"
 
 using namespace sesk;
 
@@ -88,6 +89,8 @@ struct PassPlan {
 struct Registry {
     std::vector<PlanEntry<float>> f;
     std::vector<PlanEntry<double>> d;
+    std::vector<PlaneEntry<float>> pf;  // plane passes of the two-sweep step
+    std::vector<PlaneEntry<double>> pd;
 };
 
 const Registry& registry() {
@@ -98,6 +101,7 @@ const Registry& registry() {
         register_plans_mixed(r.f, r.d);
         register_plans_256(r.f, r.d);
         register_plans_large(r.f, r.d);
+        register_planes(r.pf, r.pd);
     });
     return r;
 }
@@ -113,6 +117,24 @@ const PlanEntry<T>* find_plan(int n, int kind) {
     for (const auto& e : v)
         if (e.n == n && (e.kinds & kind)) return &e;
     return nullptr;
+}
+
+// The plane passes (one per CTAs-per-plane variant) for an nx x ny plane whose x
+// and y passes run the compiled plans px and py: the plane pass runs exactly
+// those passes' plans and radix orders.
+template <typename T>
+std::vector<const PlaneEntry<T>*> plane_candidates(int nx, int ny, const PlanEntry<T>* px, const PlanEntry<T>* py) {
+    std::vector<const PlaneEntry<T>*> out;
+    if (!px || !py) return out;
+    const auto& v = [] () -> const std::vector<PlaneEntry<T>>& {
+        if constexpr (sizeof(T) == 4) return registry().pf;
+        else return registry().pd;
+    }();
+    for (const auto& e : v)
+        if (e.nx == nx && e.ny == ny && e.xe == px->e && e.xr[0] == px->r0 && e.xr[1] == px->r1 &&
+            e.xr[2] == px->r2 && e.ye == py->e && e.yr[0] == py->r0 && e.yr[1] == py->r1 && e.yr[2] == py->r2)
+            out.push_back(&e);
+    return out;
 }
 
 // Per-stage twiddles of a compiled plan, forward order then reversed order:
@@ -266,6 +288,11 @@ struct ses_solver {
     uint32_t extra_tx = 0;         // failure-detection hook: bytes each tile barrier expects beyond its copies
     int xsel = 0;                  // pipelined contiguous-pass variant (-1: register path)
     int ssel[3] = {0, 0, 0};       // pipelined strided-pass variant per axis (-1: register path)
+    // two-sweep 3D step (plane pass with the y transforms, then the z pass) when
+    // the x-y plane fits in shared memory: the compiled plane pass (nullptr: not
+    // available for this grid) and whether steps use it
+    const void* plane = nullptr;
+    bool use_plane = false;
     ses_batch_s* batch = nullptr;  // batch this handle belongs to (its stream is the batch's)
     // long 1D line (nx > 4096, ny = nz = 1) stored as n[0] x n[1] = N1 x N2 and
     // transformed in four steps; box[0..1] and N keep the physical line
@@ -598,6 +625,48 @@ ses_status pass_s(const ses_solver* h, int axis, const void* src, void* dst, int
     return launch<T>(h, axis, mode, a, s);
 }
 
+// Plane pass of the two-sweep 3D step on `field` (PlaneMode `mode`, diagonal
+// program of p): the x pass's arguments carry the field, tables and program,
+// the y pass's the y stage twiddles and the inverse y pass's scale (1).
+template <typename T>
+ses_status pass_plane(const ses_solver* h, int mode, const XProg& p, void* field, cudaStream_t s) {
+    const PlaneEntry<T>* e = reinterpret_cast<const PlaneEntry<T>*>(h->plane);
+    if (!e) return fail(SES_EINVAL, "no plane pass for this grid");
+    PassArgs<T> ax = make_args<T>(h, 0, field, field);
+    ax.d_load = p.d_load;
+    ax.d_mid = p.d_mid;
+    ax.d_store = p.d_store;
+    ax.m_load = p.m_load;
+    ax.m_mid = p.m_mid;
+    ax.m_store = p.m_store;
+    PassArgs<T> ay = make_args<T>(h, 1, field, field);
+    ay.out_scale = 1.0;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)(h->n[2] * e->cs));  // a cluster of e->cs CTAs per z-plane
+    cfg.blockDim = dim3((unsigned)e->nt);
+    cfg.dynamicSmemBytes = e->smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[2];
+    int na = 0;
+    if (e->cs > 1) {
+        at[na].id = cudaLaunchAttributeClusterDimension;
+        at[na].val.clusterDim.x = (unsigned)e->cs;
+        at[na].val.clusterDim.y = 1;
+        at[na].val.clusterDim.z = 1;
+        ++na;
+    }
+    if (h->pdl) {
+        at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[na].val.programmaticStreamSerializationAllowed = 1;
+        ++na;
+    }
+    cfg.attrs = at;
+    cfg.numAttrs = na;
+    const cudaError_t err = cudaLaunchKernelEx(&cfg, e->k[mode], ax, ay);
+    if (err != cudaSuccess) return fail(SES_EDEVICE, std::string("plane pass launch: ") + cudaGetErrorString(err));
+    return SES_OK;
+}
+
 // Strided pass of a long line (SM_TW_*), with its potential/mask program.
 template <typename T>
 ses_status pass_tw(const ses_solver* h, const void* src, void* dst, int mode, const XProg& p, cudaStream_t s) {
@@ -661,6 +730,12 @@ ses_status interior_unit(const ses_solver* h, bool mask, cudaStream_t s) {
         p.d_load = DG_FULL;
         p.m_load = mask;
         return pass_x<T>(h, h->psi, h->psi, p, s);
+    }
+    if (h->use_plane) {  // [inv y, inv x, V (M), fwd x, fwd y] [fwd z, K/N, inv z]
+        p.d_mid = DG_FULL;
+        p.m_mid = mask;
+        SES_TRY(pass_plane<T>(h, PL_MID, p, h->psi, s));
+        return pass_s<T>(h, 2, h->psi, h->psi, SM_FUSED, 1.0, s);
     }
     p.mode = XM_MID;
     p.d_mid = DG_FULL;
@@ -740,11 +815,18 @@ ses_status enqueue_steps(ses_solver* h, int S, bool mask) {
         lastp.m_store = mask;
         return pass_x<T>(h, h->psi, h->psi, lastp, s);
     }
+    // 3D / 2D: [V/2, fwd x] [y, z] {[inv x, V (M), fwd x] [y, z]} ... [inv x, V/2 (M)];
+    // two-sweep 3D: [V/2, fwd x, fwd y] [z] {[inv y, inv x, V (M), fwd x, fwd y] [z]} ... [inv y, inv x, V/2 (M)]
     XProg start;
     start.mode = XM_START;
     start.d_load = DG_HALF;
-    SES_TRY(pass_x<T>(h, h->psi, h->psi, start, s));
-    SES_TRY(mid_axes<T>(h, s));
+    if (h->use_plane) {
+        SES_TRY(pass_plane<T>(h, PL_START, start, h->psi, s));
+        SES_TRY(pass_s<T>(h, 2, h->psi, h->psi, SM_FUSED, 1.0, s));
+    } else {
+        SES_TRY(pass_x<T>(h, h->psi, h->psi, start, s));
+        SES_TRY(mid_axes<T>(h, s));
+    }
     int interior = S - 1;
     if (interior >= kBodyUnroll) SES_TRY(ensure_body<T>(h, mask));
     while (interior >= kBodyUnroll) {
@@ -756,6 +838,7 @@ ses_status enqueue_steps(ses_solver* h, int S, bool mask) {
     end.mode = XM_END;
     end.d_store = DG_HALF;
     end.m_store = mask;
+    if (h->use_plane) return pass_plane<T>(h, PL_END, end, h->psi, s);
     return pass_x<T>(h, h->psi, h->psi, end, s);
 }
 
@@ -977,27 +1060,37 @@ ses_status profile_batch(ses_solver* h, int S, bool mask, double* out) {
             }
             return SES_OK;
         };
+        // two-sweep steps: the plane passes count as x passes (kinds 4, 0, 5), the
+        // z pass as the fused pass; the y kinds stay empty
+        auto xpass = [&](const XProg& p, int pmode) -> ses_status {
+            return h->use_plane ? pass_plane<T>(h, pmode, p, h->psi, s) : pass_x<T>(h, h->psi, h->psi, p, s);
+        };
+        auto rest = [&]() -> ses_status {
+            if (!h->use_plane) return mids();
+            SES_TRY(mark(2));
+            return pass_s<T>(h, 2, h->psi, h->psi, SM_FUSED, 1.0, s);
+        };
         XProg start;
         start.mode = XM_START;
         start.d_load = DG_HALF;
         SES_TRY(mark(4));
-        SES_TRY(pass_x<T>(h, h->psi, h->psi, start, s));
-        SES_TRY(mids());
+        SES_TRY(xpass(start, PL_START));
+        SES_TRY(rest());
         for (int k = 1; k < S; ++k) {
             XProg p;
             p.mode = XM_MID;
             p.d_mid = DG_FULL;
             p.m_mid = mask;
             SES_TRY(mark(0));
-            SES_TRY(pass_x<T>(h, h->psi, h->psi, p, s));
-            SES_TRY(mids());
+            SES_TRY(xpass(p, PL_MID));
+            SES_TRY(rest());
         }
         XProg end;
         end.mode = XM_END;
         end.d_store = DG_HALF;
         end.m_store = mask;
         SES_TRY(mark(5));
-        SES_TRY(pass_x<T>(h, h->psi, h->psi, end, s));
+        SES_TRY(xpass(end, PL_END));
         return mark(-1);
     };
     st = run();
@@ -1095,8 +1188,71 @@ int variant_count(const ses_solver* h, int axis) {
     return axis == 0 ? (int)e->xv.size() : (int)std::min<size_t>(e->sv.size(), ses_solver::kMaxVar);
 }
 
-// Selections at creation: cache, then environment overrides SES_XVAR / SES_SVAR.
+std::string plane_tune_key(const ses_solver* h) {
+    std::ostringstream k;
+    k << "sm" << h->sms << ":" << (h->prec == SES_C128 ? "c128" : "c64") << ":plane:" << h->n[0] << "x"
+      << h->n[1] << "x" << h->n[2];
+    return k.str();
+}
+
+// Plane passes of a 3D grid whose x and y axes run compiled plans they were built with.
+template <typename T>
+std::vector<const PlaneEntry<T>*> handle_planes(const ses_solver* h) {
+    if (h->long1d || h->last_axis != 2 || h->n[1] < 2) return {};
+    return plane_candidates<T>(h->n[0], h->n[1], reinterpret_cast<const PlanEntry<T>*>(h->pp[0].cp),
+                               reinterpret_cast<const PlanEntry<T>*>(h->pp[1].cp));
+}
+
+// Step form by CTAs per plane: 0 = four axis passes, cs > 0 = the plane pass of
+// that many CTAs per plane (false when the grid has none).
+template <typename T>
+bool select_plane(ses_solver* h, int cs) {
+    h->plane = nullptr;
+    h->use_plane = false;
+    if (cs <= 0) return true;
+    for (const PlaneEntry<T>* e : handle_planes<T>(h))
+        if (e->cs == cs) {
+            h->plane = e;
+            h->use_plane = true;
+            return true;
+        }
+    return false;
+}
+
+// Default step form of a grid with plane passes, from B200 measurements of
+// single-handle n^3 steps (us per step: four axis passes / plane on 1 CTA / on a
+// cluster of 2): complex128 32: 8.2 / 6.9 / 7.7, 48: 12.6 / 12.8 / 11.8,
+// 64: 14.6 / 13.1 / 11.8 (the one-CTA plane leaves 84 of 148 SMs idle on 64
+// planes); complex64 32: 9.7 / 5.9 / 7.4, 48: 12.8 / 8.5 / 9.7, 64: 12.8 / 10.5 /
+// 10.3, 96: 25.9 / 21.5 / 22.6, 128: 47.1 / 36.4 / --.
+template <typename T>
+int default_plane_cs(const ses_solver* h) {
+    auto planes = handle_planes<T>(h);
+    if (planes.empty()) return 0;
+    const int want = sizeof(T) == 8 && h->n[0] >= 48 ? 2 : 1;
+    for (auto* e : planes)
+        if (e->cs == want) return want;
+    return planes.front()->cs;
+}
+
+int plane_cs(const ses_solver* h) {
+    if (!h->use_plane || !h->plane) return 0;
+    return h->prec == SES_C128 ? reinterpret_cast<const PlaneEntry<double>*>(h->plane)->cs
+                               : reinterpret_cast<const PlaneEntry<float>*>(h->plane)->cs;
+}
+
+void apply_plane_choice(ses_solver* h, int cs) {
+    if (h->prec == SES_C128) select_plane<double>(h, cs);
+    else select_plane<float>(h, cs);
+}
+
+bool has_planes(const ses_solver* h) {
+    return h->prec == SES_C128 ? !handle_planes<double>(h).empty() : !handle_planes<float>(h).empty();
+}
+
+// Selections at creation: cache, then environment overrides SES_XVAR / SES_SVAR / SES_PLANE.
 void apply_selection(ses_solver* h) {
+    apply_plane_choice(h, h->prec == SES_C128 ? default_plane_cs<double>(h) : default_plane_cs<float>(h));
     const std::map<std::string, int> cache = read_tune_cache();
     for (int a = 0; a < 3; ++a) {
         auto it = cache.find(tune_key(h, a));
@@ -1104,9 +1260,35 @@ void apply_selection(ses_solver* h) {
         if (a == 0) h->xsel = it->second;
         else h->ssel[a] = it->second;
     }
+    if (has_planes(h)) {  // cached choice, then SES_PLANE (CTAs per plane; 0 = four axis passes)
+        auto it = cache.find(plane_tune_key(h));
+        if (it != cache.end()) apply_plane_choice(h, it->second);
+        if (const char* e = std::getenv("SES_PLANE")) apply_plane_choice(h, std::atoi(e));
+    }
     if (const char* e = std::getenv("SES_XVAR")) h->xsel = std::atoi(e);
     if (const char* e = std::getenv("SES_PDL")) h->pdl = std::atoi(e) != 0;
     if (const char* e = std::getenv("SES_SVAR")) h->ssel[1] = h->ssel[2] = std::atoi(e);
+}
+
+// Mean ms of `reps` calls of one() on the handle's stream after 2 untimed calls.
+template <class F>
+ses_status time_reps(ses_solver* h, F& one, int reps, float* ms) {
+    cudaStream_t s = h->stream;
+    for (int i = 0; i < 2; ++i) SES_TRY(one());
+    cudaEvent_t e0, e1;
+    SES_CU(cudaEventCreate(&e0));
+    SES_CU(cudaEventCreate(&e1));
+    cudaEventRecord(e0, s);
+    ses_status st = SES_OK;
+    for (int i = 0; i < reps && st == SES_OK; ++i) st = one();
+    cudaEventRecord(e1, s);
+    if (st == SES_OK) st = wait_bounded(h, 60000);
+    float t = 0.f;
+    if (st == SES_OK) cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / reps;
+    return st;
 }
 
 // Mean ms of `reps` launches of the axis's step pass on the scratch field.
@@ -1127,21 +1309,30 @@ ses_status time_axis_pass(ses_solver* h, int axis, int reps, float* ms) {
         }
         return pass_s<T>(h, axis, h->scratch, h->scratch, axis == h->last_axis ? SM_FUSED : SM_FWD, 1.0, s);
     };
-    for (int i = 0; i < 2; ++i) SES_TRY(one());
-    cudaEvent_t e0, e1;
-    SES_CU(cudaEventCreate(&e0));
-    SES_CU(cudaEventCreate(&e1));
-    cudaEventRecord(e0, s);
-    ses_status st = SES_OK;
-    for (int i = 0; i < reps && st == SES_OK; ++i) st = one();
-    cudaEventRecord(e1, s);
-    if (st == SES_OK) st = wait_bounded(h, 60000);
-    float t = 0.f;
-    if (st == SES_OK) cudaEventElapsedTime(&t, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    *ms = t / reps;
-    return st;
+    return time_reps(h, one, reps, ms);
+}
+
+// Mean ms of `reps` interior steps on the scratch field in the handle's current
+// step form (four axis passes, or plane pass + z pass).
+template <typename T>
+ses_status time_step_form(ses_solver* h, int reps, float* ms) {
+    cudaStream_t s = h->stream;
+    void* f = h->scratch;
+    auto one = [&]() -> ses_status {
+        XProg p;
+        p.mode = XM_MID;
+        p.d_mid = DG_FULL;
+        p.m_mid = h->has_mask;
+        if (h->use_plane) {
+            SES_TRY(pass_plane<T>(h, PL_MID, p, f, s));
+            return pass_s<T>(h, 2, f, f, SM_FUSED, 1.0, s);
+        }
+        SES_TRY(pass_x<T>(h, f, f, p, s));
+        SES_TRY(pass_s<T>(h, 1, f, f, SM_FWD, 1.0, s));
+        SES_TRY(pass_s<T>(h, 2, f, f, SM_FUSED, 1.0, s));
+        return pass_s<T>(h, 1, f, f, SM_INV, 1.0, s);
+    };
+    return time_reps(h, one, reps, ms);
 }
 
 template <typename T>
@@ -1168,6 +1359,24 @@ ses_status autotune_impl(ses_solver* h, int flags) {
         if (axis == 0) h->xsel = best;
         else h->ssel[axis] = best;
         chosen[tune_key(h, axis)] = best;
+    }
+    const auto planes = handle_planes<T>(h);
+    if (!planes.empty()) {  // step form: four axis passes, or a plane pass (by CTAs per plane) + z pass
+        select_plane<T>(h, 0);
+        float best_ms = 0.f;
+        SES_TRY(time_step_form<T>(h, 10, &best_ms));
+        int best = 0;
+        for (const PlaneEntry<T>* e : planes) {
+            select_plane<T>(h, e->cs);
+            float ms = 0.f;
+            SES_TRY(time_step_form<T>(h, 10, &ms));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = e->cs;
+            }
+        }
+        select_plane<T>(h, best);
+        chosen[plane_tune_key(h)] = best;
     }
     h->pipelined = saved_pipe;
     drop_graphs(h);
@@ -1205,6 +1414,12 @@ std::string plan_info_t(const ses_solver* h) {
             }
         }
         if (a < 2) o << "; ";
+    }
+    if (has_planes(h)) {
+        const int cs = plane_cs(h);
+        o << "; step: ";
+        if (cs == 0) o << "four axis passes";
+        else o << "two sweeps (x-y plane pass on " << cs << (cs == 1 ? " CTA" : " CTAs") << " per plane, z pass)";
     }
     return o.str();
 }
