@@ -13,6 +13,8 @@
 // kinetic phase, 1/N) are applied in FP64 whatever the storage precision.
 #pragma once
 
+#include <type_traits>
+
 #include "ses_fft.cuh"
 
 namespace sesk {
@@ -201,6 +203,24 @@ __device__ __forceinline__ cx<T> kinetic_full(cx<T> v, const void* kfull, long l
 template <typename T>
 __device__ __forceinline__ cx<T> kinetic_apply(cx<T> v, cx<double> dother, const cx<double>* kda64,
                                                const cx<float>* kda32, int pos, double kscale);
+
+// kinetic_apply with the axis's delta at this element fetched beforehand (kde:
+// the FP64 delta for complex128, the FP32-rounded one for complex64): the same
+// arithmetic, so passes that prefetch their tables give the same bits.
+template <typename T>
+using KinDelta = typename std::conditional<sizeof(T) == 4, cx<float>, cx<double>>::type;
+
+template <typename T>
+__device__ __forceinline__ cx<T> kinetic_apply_pre(cx<T> v, cx<double> dother, KinDelta<T> kde, double kscale) {
+    if constexpr (sizeof(T) == 4) return kinetic_conj_f(v, dmul1f(narrow<float>(dother), kde), kscale);
+    else return kinetic_conj(v, dmul1(dother, kde), kscale);
+}
+
+template <typename T>
+__device__ __forceinline__ KinDelta<T> kin_delta(const cx<double>* kda64, const cx<float>* kda32, int pos) {
+    if constexpr (sizeof(T) == 4) return kda32[pos];
+    else return kda64[pos];
+}
 
 template <int NR>
 __device__ __forceinline__ void block_reduce_store(double (&acc)[NR], double* out) {

@@ -464,6 +464,19 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
                 e = tw4_mul<T>(cconj(e), a.tb, base + pos * se);
             v[b * RF + r] = e;
         }
+    // fused pass: the line's kinetic deltas (when they fit in 32 registers a thread), fetched before the first FFT
+    cx<double> dother = mk<double>(0.0, 0.0);
+    constexpr bool kPre = MODE == SM_FUSED && E * sizeof(KinDelta<T>) <= 128;
+    KinDelta<T> kde[kPre ? E : 1];
+    if constexpr (kPre) {
+        dother = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
+        const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
+        const cx<float>* kdaf = ypass ? a.tb.kdf[1] : a.tb.kdf[2];
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) kde[b * RL + r] = kin_delta<T>(kda, kdaf, q + TL * b + r * (N / RL));
+    }
 
     rfft_plan<T, N, E, R0, R1, R2, kRev, PK>(v, q, twh, twl, x);
 
@@ -543,16 +556,21 @@ __device__ __forceinline__ void spass2_body(const A& a, long long blk, cx<T>* ti
         return;
     }
     if constexpr (MODE == SM_FUSED) {
-        const cx<double> dother = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
-        const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
-        const cx<float>* kdaf = ypass ? a.tb.kdf[1] : a.tb.kdf[2];
+        if constexpr (kPre) {
 #pragma unroll
-        for (int b = 0; b < E / RL; ++b)
+            for (int i2 = 0; i2 < E; ++i2) v[i2] = kinetic_apply_pre<T>(v[i2], dother, kde[i2], a.tb.kscale);
+        } else {
+            const cx<double> dl = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
+            const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
+            const cx<float>* kdaf = ypass ? a.tb.kdf[1] : a.tb.kdf[2];
 #pragma unroll
-            for (int r = 0; r < RL; ++r) {
-                const int pos = q + TL * b + r * (N / RL);
-                v[b * RL + r] = kinetic_apply(v[b * RL + r], dother, kda, kdaf, pos, a.tb.kscale);
-            }
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) {
+                    const int pos = q + TL * b + r * (N / RL);
+                    v[b * RL + r] = kinetic_apply(v[b * RL + r], dl, kda, kdaf, pos, a.tb.kscale);
+                }
+        }
         rfft_plan<T, N, E, R0, R1, R2, true, PK>(v, q, twh, twl, x);
         if (valid) {
 #pragma unroll

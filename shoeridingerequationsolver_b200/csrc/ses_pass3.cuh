@@ -129,11 +129,6 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
 
     for (int i = 0; i < nmine; ++i) {
         const int buf = i % NBUF;
-        const bool ok = mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i / NBUF) & 1), pa.wait_limit);
-        if (__syncthreads_or(!ok)) {
-            pipe_abort(pa, bars, NBUF, i, nmine);
-            return;
-        }
         const uint32_t t = blockIdx.x + (uint32_t)i * gridDim.x;
         const PassArgs<T>& a = f.args(t);
         const bool ypass = a.axis == 1;
@@ -144,6 +139,32 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
         const long long w = (long long)fdiv((uint32_t)sc_, a.fnu);
         const long long u = sc_ - w * a.nu;
         const long long base = u + w * a.sw;
+        int c1, c2;  // the line's other two coordinates: y-pass (x, z), z-pass (x, y)
+        if (ypass) {
+            c1 = (int)u;
+            c2 = (int)w;
+        } else {
+            c2 = (int)fdiv((uint32_t)u, a.fnx);
+            c1 = (int)(u - (long long)c2 * a.nx);
+        }
+        // fused pass: the line's kinetic deltas (when they fit in 32 registers a thread), fetched while the tile's copy is in flight
+        cx<double> dother = mk<double>(0.0, 0.0);
+        constexpr bool kPre = MODE == SM_FUSED && E * sizeof(KinDelta<T>) <= 128;
+        KinDelta<T> kde[kPre ? E : 1];
+        if constexpr (kPre) {
+            dother = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
+            const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
+            const cx<float>* kdaf = ypass ? a.tb.kdf[1] : a.tb.kdf[2];
+#pragma unroll
+            for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) kde[b * RL + r] = kin_delta<T>(kda, kdaf, q + TL * b + r * (N / RL));
+        }
+        const bool ok = mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i / NBUF) & 1), pa.wait_limit);
+        if (__syncthreads_or(!ok)) {
+            pipe_abort(pa, bars, NBUF, i, nmine);
+            return;
+        }
         XchCta<T, L> x{tile, l};
         cx<T> v[E];
 #pragma unroll
@@ -156,14 +177,6 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
         __syncthreads();  // all stage-0 reads before the tile is reused for exchanges
         rfft_plan<T, N, E, R0, R1, R2, false, kSmemTw>(v, q, twh, twl, x);
 
-        int c1, c2;
-        if (ypass) {
-            c1 = (int)u;
-            c2 = (int)w;
-        } else {
-            c2 = (int)fdiv((uint32_t)u, a.fnx);
-            c1 = (int)(u - (long long)c2 * a.nx);
-        }
         if constexpr (MODE == SM_FWD || MODE == SM_INV) {
             if (valid) {
 #pragma unroll
@@ -177,16 +190,21 @@ __device__ __forceinline__ void spass3_body(const F& f, const PipeArgs& pa) {
                     }
             }
         } else if constexpr (MODE == SM_FUSED) {
-            const cx<double> dother = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
-            const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
-            const cx<float>* kdaf = ypass ? a.tb.kdf[1] : a.tb.kdf[2];
+            if constexpr (kPre) {
 #pragma unroll
-            for (int b = 0; b < E / RL; ++b)
+                for (int i2 = 0; i2 < E; ++i2) v[i2] = kinetic_apply_pre<T>(v[i2], dother, kde[i2], a.tb.kscale);
+            } else {
+                const cx<double> dl = dmul1(a.tb.kd[0][c1], ypass ? a.tb.kd[2][c2] : a.tb.kd[1][c2]);
+                const cx<double>* kda = ypass ? a.tb.kd[1] : a.tb.kd[2];
+                const cx<float>* kdaf = ypass ? a.tb.kdf[1] : a.tb.kdf[2];
 #pragma unroll
-                for (int r = 0; r < RL; ++r) {
-                    const int pos = q + TL * b + r * (N / RL);
-                    v[b * RL + r] = kinetic_apply(v[b * RL + r], dother, kda, kdaf, pos, a.tb.kscale);
-                }
+                for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const int pos = q + TL * b + r * (N / RL);
+                        v[b * RL + r] = kinetic_apply(v[b * RL + r], dl, kda, kdaf, pos, a.tb.kscale);
+                    }
+            }
             rfft_plan<T, N, E, R0, R1, R2, true, kSmemTw>(v, q, twh, twl, x);
             if (valid) {
 #pragma unroll

@@ -66,11 +66,11 @@ constexpr size_t plane_smem() {
 // y phase, inverse (strided pass SM_INV, out_scale s): the NCOL columns x0 + xl
 // of the plane at `src` (global memory), L per round; conj, FFT in plan order
 // with the exchanges in column xl of a buffer of pitch XP (colp(xl)), then
-// out(x, pos, conj * s).
+// out(x, pos, conj * s); before_out() runs once, before the first round's outputs.
 template <typename T, int NX, int NY, int EY, int RY0, int RY1, int RY2, int L, int NCOL, int XP, bool PK, class COLP,
-          class OUT>
+          class OUT, class PRE>
 __device__ __forceinline__ void plane_y_inv(const cx<T>* __restrict__ src, int x0, COLP colp, const cx<T>* twy,
-                                            double s, OUT out) {
+                                            double s, OUT out, PRE before_out) {
     constexpr int TL = NY / EY;
     constexpr int RL = PlanShape<RY0, RY1, RY2>::last;
     const int l = threadIdx.x % L, q = threadIdx.x / L;
@@ -84,6 +84,7 @@ __device__ __forceinline__ void plane_y_inv(const cx<T>* __restrict__ src, int x
 #pragma unroll
             for (int r = 0; r < RY0; ++r) v[b * RY0 + r] = cconj(src[(q + TL * b + r * (NY / RY0)) * NX + x]);
         rfft_plan<T, NY, EY, RY0, RY1, RY2, false, PK>(v, q, twy, twy, xc);
+        if (it == 0) before_out();
 #pragma unroll
         for (int b = 0; b < EY / RL; ++b)
 #pragma unroll
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(NT, 1) plane_kernel(const PassArgs<T> ax, cons
     auto put = [&](int y, int x, cx<T> v) { P[y * PS::PITCH + PS::col(x)] = v; };
     if constexpr (MODE != PL_START) {
         plane_y_inv<T, NX, NY, EY, RY0, RY1, RY2, PS::LY, NX, PS::PITCH, PK>(
-            ax.src + gz, 0, colp, twy, ay.out_scale, [&](int x, int pos, cx<T> v) { put(pos, x, v); });
+            ax.src + gz, 0, colp, twy, ay.out_scale, [&](int x, int pos, cx<T> v) { put(pos, x, v); }, [] {});
         __syncthreads();
     }
     plane_x<T, MODE, NX, EX, RX0, RX1, RX2, NY, NT, NY, PS::SH, PS::PM, PS::PITCH, PK>(
@@ -281,6 +282,12 @@ __device__ __forceinline__ void st_cluster(uint32_t a, cx<float> v) {
 __device__ __forceinline__ void cluster_barrier() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
+// The two halves of a barrier that orders no memory: arrive (this thread has
+// started), and wait (every thread of the cluster has arrived).
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.aligned;" ::: "memory"); }
 
 // Base (shared::cluster address) of the same buffer in CTA o, o < CS, from the CS
 // bases mapped once per kernel (compile-time selects, no indexed local array).
@@ -344,16 +351,20 @@ __global__ void __launch_bounds__(NT, 1) cluster_plane_kernel(const PassArgs<T> 
         rb[o] = cluster_map(R, (uint32_t)o);
         cb[o] = cluster_map(Cb, (uint32_t)o);
     }
-    cluster_barrier();  // every CTA of the cluster runs (its buffers exist); twiddles in place
+    // every CTA of the cluster runs (its buffers exist) before any of them is
+    // written remotely: arrive now, wait before the first remote store
+    cluster_arrive_relaxed();
+    __syncthreads();  // twiddles in place
     auto colp = [&](int xl) { return Cb + xl; };
+    if constexpr (MODE == PL_START) cluster_wait();
     if constexpr (MODE != PL_START) {
         // column results (x, y) to row y of the CTA that owns it
         auto to_rows = [&](int x, int y, cx<T> v) {
             const int o = y / PS::NYC;
             st_cluster(pick_base<CS>(rb, o) + (uint32_t)((y - o * PS::NYC) * PS::PITCH + PS::col(x)) * ES, v);
         };
-        plane_y_inv<T, NX, NY, EY, RY0, RY1, RY2, PS::LY, PS::NXC, PS::CPITCH, PK>(ax.src + gz, c * PS::NXC, colp,
-                                                                                   twy, ay.out_scale, to_rows);
+        plane_y_inv<T, NX, NY, EY, RY0, RY1, RY2, PS::LY, PS::NXC, PS::CPITCH, PK>(
+            ax.src + gz, c * PS::NXC, colp, twy, ay.out_scale, to_rows, [] { cluster_wait(); });
         cluster_barrier();
     }
     // row results (x, y) to column x of the CTA that owns it
