@@ -49,8 +49,14 @@ UNIT = "grid-pt*steps/s"
 # algorithmic bytes per grid point per Strang step: 2*d*2*E + E_tab
 MODEL_BYTES = {("c128", 3): 208, ("c64", 3): 104, ("c128", 2): 144, ("c64", 2): 72, ("c128", 1): 80,
                ("c64", 1): 40}
-# bytes a step of this implementation moves per grid point (4 sweeps of psi + the table)
+# bytes a step of this implementation moves per grid point: four sweeps of psi + the
+# table; the two-sweep step (x-y plane pass + z pass, planes up to 128^2) two sweeps + the table
 ACTUAL_BYTES = {"c128": 144, "c64": 72}
+TWO_SWEEP_BYTES = {"c128": 80, "c64": 40}
+
+
+def two_sweep(plan: str) -> bool:
+    return "two sweeps" in plan
 ESIZE = {"c128": 16, "c64": 8}
 STAND_IN = ("the reference core transforms powers of two only (core/src/fft.ixx:42-44): its arm times "
             "48/96/160 at the per-point rate it reaches on 64/128/256")
@@ -261,8 +267,10 @@ def fp64_plain(ses, shapes, stream, warm=3, min_ms=300.0):
         ms = time_handle(op, stream, K, absorb)
         K = max(K, int(min_ms / max(ms / K, 1e-4)))
         ms = time_handle(op, stream, K, absorb)
+        plan = op.plan_info()
         op.close()
-        per[key] = {"ms_per_step": round(ms / K, 5), "steps_timed": K}
+        per[key] = {"ms_per_step": round(ms / K, 5), "steps_timed": K,
+                    "step_form": "two sweeps" if two_sweep(plan) else "four axis passes"}
     return per
 
 
@@ -276,6 +284,7 @@ def fp64_plain_mix(ses, specs, stream):
     npts = sum(sp["n"] ** 3 for sp in specs)
     return {"value": npts / (total_ms * 1e-3), "ms_per_step": total_ms, "dtype": "c128",
             "ms_per_step_by_size": {str(n): per[n]["ms_per_step"] for n in sorted(per)},
+            "step_form_by_size": {str(n): per[n]["step_form"] for n in sorted(per)},
             "how": "each size alone (>= 0.3 s of timed steps after 3), times the instance count"}
 
 
@@ -583,6 +592,7 @@ def fp64_plain_c5(ses, nreq, stream):
     ptsteps = sum(s["points"] * s["steps"] for s in specs)
     return {"value": ptsteps / total_s, "unit": UNIT, "dtype": "c128", "grid_pt_steps": ptsteps,
             "ms_per_step_by_shape": {k: per[k]["ms_per_step"] for k in sorted(per)},
+            "step_form_by_shape": {k: per[k]["step_form"] for k in sorted(per)},
             "how": "each distinct request shape alone (>= 0.3 s of timed steps, the first request's potential "
                    "and dt), times its requests' step counts"}
 
@@ -599,12 +609,16 @@ def single_workload(args):
     return scenes.config_c2(args.n or 256)
 
 
-def single_roofline(prof, npts, prec, peak, peak_kind, traffic_table, wname):
+def single_roofline(prof, npts, prec, peak, peak_kind, traffic_table, wname, plan=""):
     """Dominant pass of a 3D step: per-launch algorithmic bytes x -> 4E + E_tab,
-    y forward 2E, last-axis fused 4E, y inverse 2E; moved bytes 2E (+ E_tab on x)."""
+    y forward 2E, last-axis fused 4E, y inverse 2E; moved bytes 2E (+ E_tab on x).
+    Two-sweep step: the plane pass (profiled as the x pass) carries both y
+    transforms, 8E + E_tab of model bytes, and moves 2E + E_tab."""
     E = ESIZE[prec]
     per_pt = {"x_mid": 4 * E + E, "y_fwd": 2 * E, "fused": 4 * E, "y_inv": 2 * E}
     moved = {"x_mid": 3 * E, "y_fwd": 2 * E, "fused": 2 * E, "y_inv": 2 * E}
+    if two_sweep(plan):
+        per_pt["x_mid"] = 8 * E + E
     kinds = {k: prof[k] for k in per_pt if prof.get(k, 0) > 0}
     dom = max(kinds, key=kinds.get)
     alg = per_pt[dom] * npts
@@ -614,7 +628,8 @@ def single_roofline(prof, npts, prec, peak, peak_kind, traffic_table, wname):
             "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic_table.get(f"{wname}:{prec}:{dom}"), "algorithmic_bytes_per_launch": alg,
             "launch_ms": round(kinds[dom], 5), "moved_gbs": round(act, 1), "moved_frac": round(act / peak, 4),
-            "pass_ms": {k: round(v, 5) for k, v in kinds.items()}}
+            "pass_ms": {k: round(v, 5) for k, v in kinds.items()},
+            "step_form": "two sweeps" if two_sweep(plan) else "four axis passes"}
 
 
 def single_precision(ses, w, prec, W, stream, clocks_gpu, min_ms=600.0, K=None):
@@ -644,10 +659,12 @@ def single_entry(w, prec, r, peak, peak_kind, traffic_table):
     npts = w.grid.size()
     v = npts * r["K"] / (r["ms"] * 1e-3)
     mb = MODEL_BYTES[(prec, 3)]
+    moved = TWO_SWEEP_BYTES[prec] if two_sweep(r["plan"]) else ACTUAL_BYTES[prec]
     return {"precision": prec, "value": v, "ms_per_step": r["ms"] / r["K"], "steps_timed": r["K"],
             "step_model_gbs": round(mb * v / 1e9, 1), "step_frac": round(mb * v / 1e9 / peak, 4),
-            "step_moved_frac": round(ACTUAL_BYTES[prec] * v / 1e9 / peak, 4),
-            "roofline": single_roofline(r["profile"], npts, prec, peak, peak_kind, traffic_table, w.name),
+            "step_moved_bytes_per_pt": moved, "step_moved_frac": round(moved * v / 1e9 / peak, 4),
+            "roofline": single_roofline(r["profile"], npts, prec, peak, peak_kind, traffic_table, w.name,
+                                        r["plan"]),
             "clocks": r["clocks"], "plan": r["plan"]}
 
 
