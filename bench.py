@@ -58,6 +58,7 @@ TWO_SWEEP_BYTES = {"c128": 80, "c64": 40}
 def two_sweep(plan: str) -> bool:
     return "two sweeps" in plan
 ESIZE = {"c128": 16, "c64": 8}
+L2_BYTES = 126 * 2 ** 20  # B200
 STAND_IN = ("the reference core transforms powers of two only (core/src/fft.ixx:42-44): its arm times "
             "48/96/160 at the per-point rate it reaches on 64/128/256")
 
@@ -801,7 +802,8 @@ def run_ours(args):
                "n_gpus": world, "steps": r["K"], "warmup": W, "ms_per_step": ms / r["K"], "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
                "config": {"workload": w.name, "grid": list(w.grid.dims), "parallelism": f"replicas x{world}",
-                          "l2": "inputs larger than L2, no flush"},
+                          "l2": ("inputs larger than L2, no flush" if w.grid.size() * ESIZE[args.precision] > L2_BYTES
+                                 else "field smaller than L2 (the configuration's whole working set): no flush")},
                "clocks": e["clocks"], "roofline": e["roofline"], "single": e}
         if rank == 0:
             print(json.dumps(out), flush=True)
