@@ -1876,6 +1876,8 @@ struct BatchClass {
     size_t hcap[2] = {0, 0};
     cudaEvent_t staged[2] = {nullptr, nullptr};
     int stage_i = 0;
+    // two-sweep step of a 3D class (batched plane pass + z pass; nullptr: four passes)
+    const void* plane = nullptr;
 };
 
 }  // namespace
@@ -2109,6 +2111,48 @@ void share_tables(const BatchClass& c, size_t i, PassArgs<T>& a) {
         }
 }
 
+std::string batch_plane_key(const ses_batch_s* b, const BatchClass& c) {
+    std::ostringstream k;
+    k << "sm" << b->sms << ":" << (c.prec == SES_C128 ? "c128" : "c64") << ":batch-plane:" << c.n[0] << "x"
+      << c.n[1] << "x" << c.n[2];
+    return k.str();
+}
+
+// The batched plane pass of a 3D class (one CTA per plane, built for the class's
+// x and y plans), when the step form is two sweeps: by the class's shape and
+// precision only -- the batch's tuned choice, else the tune cache, else
+// SES_BATCH_PLANE (1: two sweeps), else four passes -- so a member steps the same
+// way alone and in any mix.
+template <typename T>
+const PlaneEntry<T>* class_plane_entry(const BatchClass& c) {
+    const ses_solver* h0 = c.mem[0];
+    if (!c.batched || h0->long1d || h0->last_axis != 2 || h0->n[1] < 2 || c.nmid != 3) return nullptr;
+    const PlaneEntry<T>* pe = nullptr;
+    for (const PlaneEntry<T>* e : plane_candidates<T>(h0->n[0], h0->n[1],
+                                                      reinterpret_cast<const PlanEntry<T>*>(h0->pp[0].cp),
+                                                      reinterpret_cast<const PlanEntry<T>*>(h0->pp[1].cp)))
+        if (e->cs == 1 && e->kb[PL_MID]) pe = e;
+    return pe;
+}
+
+template <typename T>
+const void* class_plane(const ses_batch_s* b, const BatchClass& c) {
+    const PlaneEntry<T>* pe = class_plane_entry<T>(c);
+    if (!pe) return nullptr;
+    int use = 0;
+    const std::string key = batch_plane_key(b, c);
+    auto it = b->sel.find(key);
+    if (it != b->sel.end()) {
+        use = it->second;
+    } else {
+        const std::map<std::string, int> cache = read_tune_cache();
+        auto jt = cache.find(key);
+        if (jt != cache.end()) use = jt->second;
+        else if (const char* env = std::getenv("SES_BATCH_PLANE")) use = std::atoi(env);
+    }
+    return use ? pe : nullptr;
+}
+
 template <typename T>
 ses_status class_upload(const ses_batch_s* b, BatchClass& c) {
     const size_t nm = c.mem.size();
@@ -2152,6 +2196,7 @@ ses_status class_upload(const ses_batch_s* b, BatchClass& c) {
                 share_tables(c, i, a);
             }
     class_select<T>(b, c);
+    c.plane = class_plane<T>(b, c);
     // tensor maps [q][member] of the members' psi for the selected strided variants
     std::vector<CUtensorMap> maps;
     bool any = false;
@@ -2210,10 +2255,44 @@ ses_status class_upload(const ses_batch_s* b, BatchClass& c) {
 // One batched pass of program `prog` over every member of the class.
 // args_ovr / maps_ovr (autotuning): the pass's per-member arguments and the
 // tensor-map table to use instead of the class's own.
+// Batched plane pass (PlaneMode pmode) over every member of class c: the x
+// program's arguments carry each member's field, tables and diagonal program,
+// the y forward pass's the y stage twiddles and the inverse y scale (1).
+template <typename T>
+ses_status class_launch_plane(const ses_batch_s* b, const BatchClass& c, int pmode, bool mask, cudaStream_t s,
+                              const void* plane = nullptr, const PassArgs<T>* axs = nullptr,
+                              const PassArgs<T>* ays = nullptr) {
+    const auto* e = reinterpret_cast<const PlaneEntry<T>*>(plane ? plane : c.plane);
+    const ses_solver* h0 = c.mem[0];
+    const size_t nm = c.mem.size();
+    const int xprog = pmode == PL_START ? BP_XSTART : (pmode == PL_MID ? BP_XMID : BP_XEND);
+    const PassArgs<T>* base = reinterpret_cast<const PassArgs<T>*>(c.dargs);
+    if (!axs) axs = base + ((size_t)xprog * 2 + (mask ? 1 : 0)) * nm;
+    if (!ays) ays = base + ((size_t)BP_MID0 * 2 + (mask ? 1 : 0)) * nm;
+    const unsigned nz = (unsigned)h0->n[2];
+    if ((unsigned long long)nz * nm >= (1ull << 31))
+        return fail(SES_EINVAL, "batch class too large: instances x planes must stay below 2^31");
+    BatchWork w{};
+    w.bpi = nz;
+    w.total = (uint32_t)(nz * nm);
+    w.fbpi = make_fastdiv(w.bpi);
+    const unsigned grid = std::min<unsigned>(w.total, (unsigned)(b->sms * std::max(1, e->kb_bps)));
+    launch_pass(h0->pdl, e->kb[pmode], grid, (unsigned)e->nt, e->smem, s, axs, ays, w);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return fail(SES_EDEVICE, std::string("batched plane pass launch: ") + cudaGetErrorString(err));
+    return SES_OK;
+}
+
 template <typename T>
 ses_status class_launch(const ses_batch_s* b, const BatchClass& c, int prog, bool mask, cudaStream_t s,
                         const PassArgs<T>* args_ovr = nullptr, const CUtensorMap* maps_ovr = nullptr) {
     const ses_solver* h0 = c.mem[0];
+    if (c.plane && !args_ovr) {  // two-sweep class: x programs are plane passes, the y passes are inside them
+        if (prog == BP_XSTART) return class_launch_plane<T>(b, c, PL_START, mask, s);
+        if (prog == BP_XMID) return class_launch_plane<T>(b, c, PL_MID, mask, s);
+        if (prog == BP_XEND) return class_launch_plane<T>(b, c, PL_END, mask, s);
+        if (prog == BP_MID0 || prog == BP_MID0 + 2) return SES_OK;
+    }
     int axis = prog < BP_NX ? 0 : (prog >= BP_LSTART ? 1 : c.mid_axis[prog - BP_MID0]);
     int mode = prog < BP_NX ? batch_xprog(prog, mask).mode : (prog >= BP_LSTART ? 0 : c.mid_mode[prog - BP_MID0]);
     if (prog >= BP_LSTART) {
@@ -2412,6 +2491,8 @@ ses_status class_autotune(ses_batch_s* b, BatchClass& c, std::map<std::string, i
     }
     const int saved_x = c.xvar;
     int saved_s[3] = {c.svar[0], c.svar[1], c.svar[2]};
+    const void* saved_plane = c.plane;  // the four-pass variants are tuned with the four-pass step
+    c.plane = nullptr;
     auto time_prog = [&](int prog, float* ms) -> ses_status {
         const PassArgs<T>* a = dargs + (prog == BP_XMID ? 0 : (size_t)(1 + prog - BP_MID0) * nm);
         SES_TRY(class_maps(c, 1, dmaps, mcap));
@@ -2460,6 +2541,44 @@ ses_status class_autotune(ses_batch_s* b, BatchClass& c, std::map<std::string, i
         c.svar[q] = saved_s[q];
         if (st == SES_OK) chosen[batch_tune_key(b, c, 1 + q)] = best;
     }
+    // step form: an interior step as four passes (with the variants just chosen)
+    // or as the plane pass and the z pass
+    const PlaneEntry<T>* pe = class_plane_entry<T>(c);
+    if (st == SES_OK && pe) {
+        const int sx = c.xvar, s0 = c.svar[0], s1 = c.svar[1], s2 = c.svar[2];
+        c.xvar = chosen[batch_tune_key(b, c, 0)];
+        for (int q = 0; q < 3; ++q) c.svar[q] = chosen[batch_tune_key(b, c, 1 + q)];
+        auto time_unit = [&](bool plane, float* ms) -> ses_status {
+            SES_TRY(class_maps(c, 1, dmaps, mcap));
+            auto unit = [&]() -> ses_status {
+                if (plane) SES_TRY(class_launch_plane<T>(b, c, PL_MID, true, b->stream, pe, dargs, dargs + nm));
+                else SES_TRY(class_launch<T>(b, c, BP_XMID, true, b->stream, dargs, dmaps));
+                for (int q = 0; q < c.nmid; ++q) {
+                    if (plane && q != 1) continue;  // the y passes run inside the plane pass
+                    SES_TRY(class_launch<T>(b, c, BP_MID0 + q, true, b->stream, dargs + (size_t)(1 + q) * nm, dmaps));
+                }
+                return SES_OK;
+            };
+            SES_TRY(unit());
+            SES_CU(cudaEventRecord(e0, b->stream));
+            for (int r = 0; r < 3; ++r) SES_TRY(unit());
+            SES_CU(cudaEventRecord(e1, b->stream));
+            SES_TRY(batch_wait(b, 60000));
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            *ms = t / 3;
+            return SES_OK;
+        };
+        float four = 0.f, two = 0.f;
+        st = time_unit(false, &four);
+        if (st == SES_OK) st = time_unit(true, &two);
+        if (st == SES_OK) chosen[batch_plane_key(b, c)] = two < four ? 1 : 0;
+        c.xvar = sx;
+        c.svar[0] = s0;
+        c.svar[1] = s1;
+        c.svar[2] = s2;
+    }
+    c.plane = saved_plane;
     cleanup();
     return st;
 }
@@ -3180,6 +3299,11 @@ ses_status ses_batch_info(ses_batch b, char* buf, size_t len) {
           << (c->prec == SES_C128 ? "c128" : "c64") << " members=" << c->mem.size();
         if (!c->batched) {
             o << " member-by-member";
+            continue;
+        }
+        if (c->plane) {  // two sweeps: the plane pass replaces the x and y passes
+            o << " plane";
+            o << " s1=" << (c->svar[1] >= 0 ? "pipe" + std::to_string(c->svar[1]) : std::string("reg"));
             continue;
         }
         o << " x=" << (c->xvar >= 0 ? "pipe" + std::to_string(c->xvar) : std::string("reg"));

@@ -214,14 +214,38 @@ __device__ __forceinline__ void plane_x(const PassArgs<T>& a, int z, int y0, cx<
     }
 }
 
+// Plane z of the field of `ax` through the whole plane buffer P (element (x, y)
+// at P[y PITCH + col(x)]: rows are x-lines, columns y-lines); s: the inverse y
+// pass's scale.  In place: the plane is read whole before any of it is written.
+template <typename T, int MODE, int NX, int EX, int RX0, int RX1, int RX2, int NY, int EY, int RY0, int RY1, int RY2,
+          int NT>
+__device__ __forceinline__ void plane_body(const PassArgs<T>& ax, double s, int z, cx<T>* P, const cx<T>* twx,
+                                           const cx<T>* twy) {
+    using PS = PlaneShape<T, NX, EX, NY, EY, NT>;
+    constexpr bool PK = sizeof(T) == 4;  // complex64: interleaved hi/lo twiddles
+    const long long gz = (long long)z * NX * NY;
+    auto colp = [&](int x) { return P + PS::col(x); };
+    auto put = [&](int y, int x, cx<T> v) { P[y * PS::PITCH + PS::col(x)] = v; };
+    if constexpr (MODE != PL_START) {
+        plane_y_inv<T, NX, NY, EY, RY0, RY1, RY2, PS::LY, NX, PS::PITCH, PK>(
+            ax.src + gz, 0, colp, twy, s, [&](int x, int pos, cx<T> v) { put(pos, x, v); }, [] {});
+        __syncthreads();
+    }
+    plane_x<T, MODE, NX, EX, RX0, RX1, RX2, NY, NT, NY, PS::SH, PS::PM, PS::PITCH, PK>(
+        ax, z, 0, P, twx, [&](int y, int pos, cx<T> v) { put(y, pos, v); });
+    if constexpr (MODE != PL_END) {
+        __syncthreads();
+        plane_y_fwd<T, NX, NY, EY, RY0, RY1, RY2, PS::LY, NX, PS::PITCH, PK>(ax.dst + gz, 0, colp, twy);
+    }
+}
+
 // One CTA per z-plane (grid = nz).  ax: the x pass's arguments (field, tables,
 // diagonal program, x stage twiddles); ay: the y stage twiddles and the inverse
-// y pass's scale.  In place: a CTA reads its whole plane before it writes any of it.
+// y pass's scale.
 template <typename T, int MODE, int NX, int EX, int RX0, int RX1, int RX2, int NY, int EY, int RY0, int RY1, int RY2,
           int NT>
 __global__ void __launch_bounds__(NT, 1) plane_kernel(const PassArgs<T> ax, const PassArgs<T> ay) {
     using PS = PlaneShape<T, NX, EX, NY, EY, NT>;
-    constexpr bool PK = sizeof(T) == 4;  // complex64: interleaved hi/lo twiddles
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T>* P = reinterpret_cast<cx<T>*>(smraw);
     cx<T>* twx = reinterpret_cast<cx<T>*>(smraw + PS::plane_bytes);
@@ -230,21 +254,34 @@ __global__ void __launch_bounds__(NT, 1) plane_kernel(const PassArgs<T> ax, cons
     TwStage<T, RX0, RX1, RX2>::load(twx, ax.stw, ax.stwl);
     TwStage<T, RY0, RY1, RY2>::load(twy, ay.stw, ay.stwl);
     __syncthreads();
-    const int z = blockIdx.x;
-    const long long gz = (long long)z * NX * NY;
-    // element (x, y) of the plane at P[y PITCH + col(x)]: rows are x-lines, columns y-lines
-    auto colp = [&](int x) { return P + PS::col(x); };
-    auto put = [&](int y, int x, cx<T> v) { P[y * PS::PITCH + PS::col(x)] = v; };
-    if constexpr (MODE != PL_START) {
-        plane_y_inv<T, NX, NY, EY, RY0, RY1, RY2, PS::LY, NX, PS::PITCH, PK>(
-            ax.src + gz, 0, colp, twy, ay.out_scale, [&](int x, int pos, cx<T> v) { put(pos, x, v); }, [] {});
-        __syncthreads();
+    plane_body<T, MODE, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, NT>(ax, ay.out_scale, (int)blockIdx.x, P, twx,
+                                                                         twy);
+}
+
+// Batched plane pass: the planes of every member of a class (one shape, one
+// plan), work item t = member w.bpi + z (w.bpi = nz), CTAs walking the items
+// grid-stride; the class's stage twiddles (shared by its members) are loaded
+// once per CTA.  axs / ays: per-member x-program and y-pass arguments.
+template <typename T, int MODE, int NX, int EX, int RX0, int RX1, int RX2, int NY, int EY, int RY0, int RY1, int RY2,
+          int NT>
+__global__ void __launch_bounds__(NT, 1)
+    plane_batch_kernel(const PassArgs<T>* __restrict__ axs, const PassArgs<T>* __restrict__ ays, const BatchWork w) {
+    using PS = PlaneShape<T, NX, EX, NY, EY, NT>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T>* P = reinterpret_cast<cx<T>*>(smraw);
+    cx<T>* twx = reinterpret_cast<cx<T>*>(smraw + PS::plane_bytes);
+    cx<T>* twy = reinterpret_cast<cx<T>*>(smraw + PS::plane_bytes + TwStage<T, RX0, RX1, RX2>::bytes);
+    pdl_wait();
+    if (blockIdx.x < w.total) {
+        TwStage<T, RX0, RX1, RX2>::load(twx, axs[0].stw, axs[0].stwl);
+        TwStage<T, RY0, RY1, RY2>::load(twy, ays[0].stw, ays[0].stwl);
     }
-    plane_x<T, MODE, NX, EX, RX0, RX1, RX2, NY, NT, NY, PS::SH, PS::PM, PS::PITCH, PK>(
-        ax, z, 0, P, twx, [&](int y, int pos, cx<T> v) { put(y, pos, v); });
-    if constexpr (MODE != PL_END) {
-        __syncthreads();
-        plane_y_fwd<T, NX, NY, EY, RY0, RY1, RY2, PS::LY, NX, PS::PITCH, PK>(ax.dst + gz, 0, colp, twy);
+    __syncthreads();
+    for (uint32_t t = blockIdx.x; t < w.total; t += gridDim.x) {
+        const uint32_t m = fdiv(t, w.fbpi);
+        plane_body<T, MODE, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, NT>(axs[m], ays[m].out_scale,
+                                                                             (int)(t - m * w.bpi), P, twx, twy);
+        __syncthreads();  // the plane buffer is free for the next item
     }
 }
 
@@ -383,6 +420,8 @@ __global__ void __launch_bounds__(NT, 1) cluster_plane_kernel(const PassArgs<T> 
 
 template <typename T>
 using PlaneKernel = void (*)(const PassArgs<T>, const PassArgs<T>);
+template <typename T>
+using PlaneBatchKernel = void (*)(const PassArgs<T>*, const PassArgs<T>*, const BatchWork);
 
 // A compiled plane pass: the x and y plans it was built with (the solver uses it
 // only when its own x and y plans are these), threads and shared memory.
@@ -394,6 +433,9 @@ struct PlaneEntry {
     int cs = 1;  // CTAs per plane (a thread-block cluster when > 1)
     size_t smem = 0;
     PlaneKernel<T> k[3] = {nullptr, nullptr, nullptr};  // by PlaneMode
+    // batched form (one-CTA planes only): every member of a class, by PlaneMode
+    PlaneBatchKernel<T> kb[3] = {nullptr, nullptr, nullptr};
+    int kb_bps = 0;  // resident CTAs per SM
 };
 
 // Plane pass entry with NT threads per CTA and CS CTAs per plane (1: plane_kernel,
@@ -419,6 +461,12 @@ PlaneEntry<T> make_plane_entry() {
         p.k[PL_START] = plane_kernel<T, PL_START, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, NT>;
         p.k[PL_MID] = plane_kernel<T, PL_MID, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, NT>;
         p.k[PL_END] = plane_kernel<T, PL_END, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, NT>;
+        p.kb[PL_START] = plane_batch_kernel<T, PL_START, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, NT>;
+        p.kb[PL_MID] = plane_batch_kernel<T, PL_MID, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, NT>;
+        p.kb[PL_END] = plane_batch_kernel<T, PL_END, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, NT>;
+        for (auto k : p.kb) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessorWithFlags(&p.kb_bps, p.kb[PL_MID], NT, p.smem,
+                                                              cudaOccupancyDefault);
     } else {
         p.smem = cluster_plane_smem<T, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, CS, NT>();
         p.k[PL_START] = cluster_plane_kernel<T, PL_START, NX, EX, RX0, RX1, RX2, NY, EY, RY0, RY1, RY2, CS, NT>;
