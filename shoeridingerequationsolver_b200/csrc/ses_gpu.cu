@@ -1232,7 +1232,7 @@ int default_plane_cs(const ses_solver* h) {
     const int want = sizeof(T) == 8 && h->n[0] >= 48 ? 2 : 1;
     for (auto* e : planes)
         if (e->cs == want) return want;
-    return planes.front()->cs;
+    return 0;  // other variants only when the autotuner or SES_PLANE picks them
 }
 
 int plane_cs(const ses_solver* h) {

@@ -7,7 +7,8 @@
 // Not built, slower than four axis passes (us per n^3 step, four passes first):
 // complex128 96^2 on 1 / 2 / 4 CTAs (30.1 vs 35.0 / 40.2 / 40.3), 128^2 on 4
 // (57.8 vs 71.3); complex64 128^2 on 2 / 4 (47.1 vs 43.3 / 55.3, one CTA 36.4),
-// 160^2 on 4 (92.1 vs 112.8).
+// 160^2 on 4 (92.1 vs 112.8), 256^2 on 8 (169 KB per CTA: 310 vs 470 us, C2's grid; the
+// same bits as the four passes).
 #include "ses_plane.cuh"
 
 namespace sesk {
