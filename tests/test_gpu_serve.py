@@ -50,7 +50,11 @@ def run_all(srv, specs):
 
 
 @pytest.mark.gpu
-def test_serve_alone_equals_mix_and_oracle(ses, oracle):
+@pytest.mark.parametrize("batch_plane", ["0", "1"])
+def test_serve_alone_equals_mix_and_oracle(ses, oracle, monkeypatch, batch_plane):
+    """batch_plane "1": the 3D classes step in the two-sweep form (batched plane
+    pass + z pass), chosen by shape, so alone and in the mix alike."""
+    monkeypatch.setenv("SES_BATCH_PLANE", batch_plane)
     a = spec(ses, (32, 32, 32), 8.0, 1, nsteps=250, every=100)
     others = [spec(ses, (48, 48, 48), 9.0, 2, nsteps=130, every=50),
               spec(ses, (64, 64, 1), 10.0, 3, nsteps=370, every=100),
