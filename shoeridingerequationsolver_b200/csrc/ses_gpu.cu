@@ -3230,7 +3230,12 @@ ses_status ses_batch_run(ses_batch b, const double* const* psi_in, int nsteps, i
     SES_TRY(batch_refresh(b));
     std::map<const ses_solver*, int> index;
     for (int i = 0; i < count; ++i) index[b->members[i]] = i;
-    // largest class first: its steps start while the others are still uploading
+    // largest class first.  The copies of the class streams share the PCIe link
+    // (the copy engines interleave them), so the classes finish their uploads at
+    // about the same time and their readbacks queue at the end; chaining the
+    // uploads class by class, starting a smaller class first and holding the
+    // smallest classes' steps back to overlap the largest one's readback did not
+    // shorten the call (measured on B200 with the batched sweep, 0.76-0.77 s either way)
     std::vector<BatchClass*> order(b->classes.begin(), b->classes.end());
     std::stable_sort(order.begin(), order.end(), [](const BatchClass* x, const BatchClass* y) {
         return (double)x->mem.size() * x->n[0] * x->n[1] * x->n[2] > (double)y->mem.size() * y->n[0] * y->n[1] * y->n[2];
