@@ -694,12 +694,12 @@ void set_attrs_prec() {
     for (int m = SM_FWD; m <= SM_REDUCE; ++m) set_smem_attr(skernel<T>(m));
 }
 
-void init_kernel_attrs() {
-    static bool done = false;
-    if (done) return;
-    set_attrs_prec<float>();
-    set_attrs_prec<double>();
-    done = true;
+void init_kernel_attrs() {  // once per process; handles may be created from several threads
+    static std::once_flag once;
+    std::call_once(once, [] {
+        set_attrs_prec<float>();
+        set_attrs_prec<double>();
+    });
 }
 
 // y/z part of one step: fwd y, fused z, inv y (3D) or fused y (2D) or fused z.
