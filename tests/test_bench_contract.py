@@ -41,3 +41,28 @@ def test_reference_arm_line_and_no_device_library():
     args = bench.parse_args(["--instances", "3"])
     specs = bench.c4_all_specs(args, 1)
     assert line["config"] == bench.c4_config(specs, 1, args)
+
+
+def test_single_roofline_follows_the_step_form():
+    """The single-instance roofline credits the plane pass of the two-sweep form
+    with both y transforms (8E + E_tab model bytes, 2E + E_tab moved) and the
+    four-pass x pass with 4E + E_tab (3E moved); the dominant launch is the
+    slowest kind profiled."""
+    import bench
+    npts = 64 ** 3
+    prof_two = {"x_mid": 0.010, "fused": 0.006}
+    prof_four = {"x_mid": 0.006, "y_fwd": 0.003, "fused": 0.005, "y_inv": 0.003}
+    two = bench.single_roofline(prof_two, npts, "c128", 6537.0, "measured", {}, "c1",
+                                "x:64 ...; step: two sweeps (x-y plane pass on 2 CTAs per plane, z pass)")
+    four = bench.single_roofline(prof_four, npts, "c128", 6537.0, "measured", {}, "c1",
+                                 "x:64 ...; step: four axis passes")
+    E = 16
+    assert two["kernel"] == "x_mid" and two["step_form"] == "two sweeps"
+    assert two["algorithmic_bytes_per_launch"] == (8 * E + E) * npts
+    assert abs(two["achieved"] - (8 * E + E) * npts / 0.010e-3 / 1e9) < 0.2
+    assert abs(two["moved_gbs"] - 3 * E * npts / 0.010e-3 / 1e9) < 0.2
+    assert four["kernel"] == "x_mid" and four["step_form"] == "four axis passes"
+    assert four["algorithmic_bytes_per_launch"] == (4 * E + E) * npts
+    assert bench.two_sweep("step: two sweeps (x-y plane pass on 1 CTA per plane, z pass)")
+    assert not bench.two_sweep("step: four axis passes")
+    assert bench.TWO_SWEEP_BYTES["c128"] == 80 and bench.ACTUAL_BYTES["c128"] == 144
